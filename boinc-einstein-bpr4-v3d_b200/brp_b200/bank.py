@@ -1,0 +1,78 @@
+"""Bank search: a whole orbital bank over one or more series (possibly of
+different lengths) in one captured CUDA graph -- the batched form of the
+reference's bank loop (src/workunit_main.cpp:77-93)."""
+import ctypes
+
+import numpy as np
+
+from ._lib import CANDIDATE, BrpError, Params, check, lib, ptr
+
+
+class Bank:
+    def __init__(self, lengths, unpadded, max_templates, capacity=4096, device=-1):
+        L = lib()
+        self._b = None
+        self.n = np.ascontiguousarray(lengths, dtype=np.uint32)
+        self.unpadded = np.ascontiguousarray(unpadded, dtype=np.uint32)
+        self.max_templates = int(max_templates)
+        self.capacity = int(capacity)
+        b = ctypes.c_void_p()
+        st = L.brp_cuda_bank_create(self.n.size, ptr(self.n), ptr(self.unpadded), max_templates, capacity, device,
+                                    ctypes.byref(b))
+        check(st, lambda: L.brp_cuda_bank_last_error(None).decode())
+        self._b = b
+        self._out = np.empty(0, CANDIDATE)
+
+    def _err(self):
+        return lib().brp_cuda_bank_last_error(self._b).decode()
+
+    def close(self):
+        if self._b:
+            lib().brp_cuda_bank_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        self.close()
+
+    def set_series(self, index, series):
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        if x.size != self.unpadded[index]:
+            raise BrpError(4, "series length mismatch")
+        check(lib().brp_cuda_bank_set_series(self._b, index, ptr(x)), self._err)
+
+    def run(self, templates, series_of=None, out=None):
+        """Searches every template; returns (candidates per template, counts, status).
+        Raises BrpError when a template overflowed or resampled out of range."""
+        count = len(templates)
+        arr = (Params * count)(*templates)
+        so = np.zeros(count, np.uint32) if series_of is None else np.ascontiguousarray(series_of, dtype=np.uint32)
+        counts = np.zeros(count, np.uint32)
+        status = np.zeros(count, np.uint32)
+        cap = count * self.capacity
+        if out is None:
+            if self._out.size < cap:
+                self._out = np.empty(cap, CANDIDATE)
+            out = self._out
+        st = lib().brp_cuda_bank_run(self._b, arr, ptr(so), count, ptr(out), out.size, ptr(counts), ptr(status))
+        if st and st != 2:
+            check(st, self._err)
+        kept = np.minimum(counts, self.capacity)
+        offs = np.concatenate([[0], np.cumsum(kept)])
+        result = [out[offs[t]:offs[t + 1]].copy() for t in range(count)]
+        if st:
+            e = BrpError(st, self._err())
+            e.counts, e.status, e.candidates = counts, status, result
+            raise e
+        return result, counts, status
+
+    def launch(self):
+        """Replays the last run's graph on the device only (no copies, no wait)."""
+        check(lib().brp_cuda_bank_launch(self._b), self._err)
+
+    @property
+    def stream(self):
+        return lib().brp_cuda_bank_stream(self._b)
+
+    @property
+    def kernels_per_run(self):
+        return int(lib().brp_cuda_bank_kernels_per_run(self._b))

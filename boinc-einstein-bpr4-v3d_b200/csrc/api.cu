@@ -1,0 +1,670 @@
+// C ABI of the CUDA backend (include/brp_cuda.h): the per-template context that
+// replaces src/vulkan.cpp behind brp::GPU, and the bank extension that runs a
+// whole orbital bank as one captured CUDA graph.
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+#include "brp_internal.h"
+
+using namespace brp;
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+double cpu_ms_now() {
+    timespec t{};
+    clock_gettime(CLOCK_PROCESS_CPUTIME_ID, &t);
+    return t.tv_sec * 1000.0 + t.tv_nsec / 1e6;
+}
+
+// Waits for `ev` with a deadline instead of an unbounded blocking wait.
+cudaError_t wait_event(cudaEvent_t ev, double seconds, bool* timed_out) {
+    *timed_out = false;
+    auto start = std::chrono::steady_clock::now();
+    for (int spin = 0;; ++spin) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e != cudaErrorNotReady) return e;
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count() > seconds) {
+            *timed_out = true;
+            return cudaErrorNotReady;
+        }
+        if (spin > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+constexpr double kWaitSeconds = 300.0;
+
+bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+
+}  // namespace
+
+struct brp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    brp_params base{};
+    uint32_t wg = 0, tile = 0, batch = 0, opt = 0;
+    bool fused = false;
+    std::vector<brp_params> templates;
+    LengthPlan lp;
+    std::vector<void*> allocations;
+    uint64_t allocated = 0;
+    // device buffers
+    float* d_input = nullptr;
+    const float** d_inputs = nullptr;
+    brp_params* d_params = nullptr;
+    float2* d_work = nullptr;
+    float* d_power = nullptr;
+    double* d_partial = nullptr;
+    float* d_mean = nullptr;
+    uint32_t* d_status = nullptr;
+    uint32_t* d_counts = nullptr;
+    brp_candidate* d_cands = nullptr;
+    float* d_raw = nullptr;
+    float2* d_fft = nullptr;
+    float* d_summed = nullptr;
+    float2* d_a = nullptr;
+    float2* d_b = nullptr;
+    std::vector<cudaEvent_t> events;
+    uint32_t last_count = 0;
+    double last_stage_ms[4] = {0, 0, 0, 0};
+    std::string error;
+
+    int fail(int code, const std::string& msg) {
+        error = msg;
+        g_thread_error = msg;
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return BRP_OK;
+        return fail(BRP_E_RUNTIME, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    template <class T>
+    int alloc(T** p, size_t count, const char* what) {
+        size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        if (cudaMalloc(reinterpret_cast<void**>(p), bytes) != cudaSuccess)
+            return fail(BRP_E_RUNTIME, std::string("cudaMalloc failed: ") + what);
+        allocations.push_back(*p);
+        allocated += bytes;
+        return BRP_OK;
+    }
+    ~brp_ctx() {
+        if (device >= 0) cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto e : events) cudaEventDestroy(e);
+        for (auto p : allocations) cudaFree(p);
+        free_length_plan(lp);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static int set_thread_error(int code, const std::string& m) {
+    g_thread_error = m;
+    return code;
+}
+
+// Validation of src/vulkan.cpp:110-122 and :278-284 (flag combinations, limits).
+static std::string validate_options(const brp_params& p, const brp_options& o) {
+    const bool stockham = o.flags & BRP_OPT_STOCKHAM, packed = o.flags & BRP_OPT_PACKED;
+    const bool radix8 = o.flags & BRP_OPT_RADIX8, fused_power = o.flags & BRP_OPT_FUSED_POWER;
+    const bool radix8_store = o.flags & BRP_OPT_RADIX8_STORE;
+    if (fused_power && !packed) return "fused power requires packed real FFT";
+    if (radix8_store && !radix8) return "paired-store radix 8 requires radix 8";
+    if (radix8 && (!stockham || o.tile)) return "radix8 requires Stockham without a shared tile";
+    uint32_t fft_n = packed ? p.n / 2 : p.n;
+    uint32_t base = is_pow2(fft_n) ? fft_n : fft_n / 3;
+    if (o.tile > base) return "FFT tile exceeds radix-2 block";
+    if (stockham && o.tile) return "Stockham requires --tile 0";
+    if (!o.workgroup || o.workgroup > 256 || !o.batch || o.batch > 64 ||
+        (o.tile && (!is_pow2(o.tile) || o.tile < 64 || o.tile > 4096 || o.tile > p.n)))
+        return "invalid workgroup, FFT tile, or batch";
+    return "";
+}
+
+static std::string validate_template(const brp_params& base, const brp_params& next) {
+    // src/vulkan.cpp:271-273.
+    if ((next.flags & 6u) != (base.flags & 6u)) return "arithmetic specialization changed; rebuild pipelines";
+    if (next.n != base.n || next.unpadded != base.unpadded || next.fundamental != base.fundamental ||
+        next.harmonic != base.harmonic || next.capacity != base.capacity || !next.steps || next.steps > next.unpadded)
+        return "template dimensions changed; rebuild resources";
+    return "";
+}
+
+static std::string validate_dims(const brp_params& p) {
+    if (p.n < 64 || p.n > 3u * (1u << 22) || !(is_pow2(p.n) || (p.n % 3 == 0 && is_pow2(p.n / 3))))
+        return "series length must be 2^k or 3*2^k in 64..3*2^22";
+    if (p.unpadded < 2 || p.unpadded > p.n) return "invalid unpadded length";
+    if (!p.steps || p.steps > p.unpadded) return "invalid resampled length";
+    if (p.fundamental > p.n / 2 || p.harmonic > p.n / 2) return "harmonic search range exceeds the spectrum";
+    if (!p.capacity) return "zero candidate capacity";
+    return "";
+}
+
+extern "C" const char* brp_cuda_last_error(const brp_ctx* ctx) {
+    return ctx ? ctx->error.c_str() : g_thread_error.c_str();
+}
+
+extern "C" int brp_cuda_create(const brp_params* params, const float* input, uint32_t unpadded,
+                               const brp_options* options, brp_ctx** out) {
+    if (!params || !input || !options || !out) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    *out = nullptr;
+    brp_params p = *params;
+    std::string v = validate_options(p, *options);
+    if (v.empty()) v = validate_dims(p);
+    if (v.empty() && unpadded != p.unpadded) v = "input length mismatch";
+    if (!v.empty()) return set_thread_error(BRP_E_RUNTIME, v);
+    auto* c = new (std::nothrow) brp_ctx;
+    if (!c) return set_thread_error(BRP_E_RUNTIME, "out of host memory");
+    c->device = options->device;
+    if (c->device < 0) cudaGetDevice(&c->device);
+    int st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) { std::string m = c->error; delete c; return set_thread_error(st, m); }
+    if ((st = c->cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
+        std::string m = c->error; delete c; return set_thread_error(st, m);
+    }
+    c->base = p;
+    if (options->flags & BRP_OPT_PACKED) c->base.flags |= BRP_FLAG_PACKED;
+    c->wg = options->workgroup; c->tile = options->tile; c->batch = options->batch; c->opt = options->flags;
+    std::string e = make_length_plan(p.n, c->lp, c->stream);
+    if (!e.empty()) { delete c; return set_thread_error(BRP_E_RUNTIME, e); }
+    c->fused = c->lp.fused && !(options->flags & BRP_OPT_PLAIN);
+    const uint32_t B = c->batch, M = c->lp.M, cap = p.capacity;
+    const uint32_t slots = c->fused ? B : 1;
+    auto cleanup = [&](int code) { std::string m = c->error; delete c; return set_thread_error(code, m); };
+    if ((st = c->alloc(&c->d_input, unpadded, "input")) || (st = c->alloc(&c->d_inputs, B, "input table")) ||
+        (st = c->alloc(&c->d_params, B, "params")) || (st = c->alloc(&c->d_work, size_t(slots) * M, "work")) ||
+        (st = c->alloc(&c->d_power, size_t(slots) * M, "power")) ||
+        (st = c->alloc(&c->d_partial, size_t(slots) * std::max<uint32_t>(c->fused ? c->lp.blocks1() : (p.unpadded + 255) / 256, 1), "partial")) ||
+        (st = c->alloc(&c->d_mean, B, "mean")) || (st = c->alloc(&c->d_status, B, "status")) ||
+        (st = c->alloc(&c->d_counts, B, "counts")) || (st = c->alloc(&c->d_cands, size_t(B) * cap, "candidates")) ||
+        (st = c->alloc(&c->d_raw, p.unpadded, "resampled")) || (st = c->alloc(&c->d_fft, size_t(M) + 1, "fft")) ||
+        (st = c->alloc(&c->d_summed, size_t(5) * p.fundamental, "summed")))
+        return cleanup(st);
+    if (!c->fused && ((st = c->alloc(&c->d_a, M, "fft a")) || (st = c->alloc(&c->d_b, M, "fft b")))) return cleanup(st);
+    c->allocated += c->lp.tables_bytes;
+    if ((st = c->cuda(cudaMemcpy(c->d_input, input, size_t(unpadded) * 4, cudaMemcpyHostToDevice), "input upload")))
+        return cleanup(st);
+    std::vector<const float*> ptrs(B, c->d_input);
+    if ((st = c->cuda(cudaMemcpy(c->d_inputs, ptrs.data(), B * sizeof(void*), cudaMemcpyHostToDevice), "input table")))
+        return cleanup(st);
+    c->events.resize(5 * B);
+    for (auto& ev : c->events)
+        if ((st = c->cuda(cudaEventCreate(&ev), "cudaEventCreate"))) { ev = nullptr; return cleanup(st); }
+    c->templates.assign(1, c->base);
+    *out = c;
+    return BRP_OK;
+}
+
+extern "C" void brp_cuda_destroy(brp_ctx* ctx) { delete ctx; }
+
+extern "C" int brp_cuda_set_templates(brp_ctx* c, const brp_params* t, uint32_t count) {
+    if (!c || !t) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (!count || count > c->batch) return c->fail(BRP_E_RUNTIME, "template batch exceeds retained result capacity");
+    std::vector<brp_params> next(t, t + count);
+    for (auto& p : next) {
+        std::string v = validate_template(c->base, p);
+        if (!v.empty()) return c->fail(BRP_E_RUNTIME, v);
+        // Dimensions stay the constructor's; the remaining fields follow the template
+        // (src/vulkan.cpp:274-275).
+        brp_params q = c->base;
+        q.steps = p.steps; q.tau = p.tau; q.omega = p.omega; q.psi = p.psi; q.dt = p.dt; q.step_inv = p.step_inv;
+        q.s0 = p.s0; q.window = p.window;
+        std::memcpy(q.threshold, p.threshold, sizeof q.threshold);
+        p = q;
+    }
+    c->templates = next;
+    return BRP_OK;
+}
+
+static FusedArgs fused_args(brp_ctx* c, uint32_t count) {
+    FusedArgs a{};
+    const LengthPlan& lp = c->lp;
+    a.inputs = c->d_inputs;
+    a.params = c->d_params;
+    a.n = lp.n; a.M = lp.M; a.L1 = lp.L1; a.L2 = lp.L2; a.C = lp.C; a.R = lp.R;
+    a.plan1[0] = lp.plan1.count; a.plan2[0] = lp.plan2.count;
+    for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
+    a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
+    a.work = c->d_work; a.work_stride = lp.M;
+    a.power = c->d_power; a.power_stride = lp.M;
+    a.partial = c->d_partial; a.partial_stride = lp.blocks1();
+    a.mean = c->d_mean; a.status = c->d_status; a.counts = c->d_counts; a.cands = c->d_cands;
+    a.capacity = c->base.capacity;
+    a.snap = int(count) - 1;
+    a.snap_raw = c->d_raw; a.snap_fft = c->d_fft; a.snap_summed = c->d_summed;
+    return a;
+}
+
+extern "C" int brp_cuda_run(brp_ctx* c, brp_timings* timings, double* template_stage_ms) {
+    if (!c) return set_thread_error(BRP_E_ARGUMENT, "null context");
+    int st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    auto start = std::chrono::steady_clock::now();
+    double cpu0 = cpu_ms_now();
+    const uint32_t count = uint32_t(c->templates.size());
+    const brp_params& last = c->templates.back();
+    cudaStream_t s = c->stream;
+    auto submit0 = std::chrono::steady_clock::now();
+    if ((st = c->cuda(cudaMemcpyAsync(c->d_params, c->templates.data(), count * sizeof(brp_params),
+                                      cudaMemcpyHostToDevice, s), "params upload")))
+        return st;
+    cudaMemsetAsync(c->d_counts, 0, count * sizeof(uint32_t), s);
+    cudaMemsetAsync(c->d_status, 0, count * sizeof(uint32_t), s);
+    cudaMemsetAsync(c->d_summed, 0, size_t(5) * last.fundamental * sizeof(float), s);
+    cudaEvent_t* ev = c->events.data();
+    if (c->fused) {
+        FusedArgs a = fused_args(c, count);
+        uint32_t span = 0;
+        for (auto& p : c->templates) span = std::max(span, std::max(p.fundamental, p.harmonic + 8));
+        cudaEventRecord(ev[0], s);
+        launch_fused_pass1(a, c->lp, count, s);
+        cudaEventRecord(ev[1], s);
+        launch_fused_pass2(a, c->lp, count, s);
+        cudaEventRecord(ev[2], s);
+        cudaEventRecord(ev[3], s);
+        launch_fused_harmonic(a, c->lp, count, span, s);
+        cudaEventRecord(ev[4], s);
+    } else {
+        for (uint32_t t = 0; t < count; ++t) {
+            PlainArgs a{};
+            a.input = c->d_input; a.p = c->templates[t]; a.lp = &c->lp;
+            a.raw = c->d_raw; a.partial = c->d_partial; a.mean = c->d_mean; a.a = c->d_a; a.b = c->d_b;
+            a.fft = c->d_fft; a.power = c->d_power; a.summed = c->d_summed;
+            a.status = c->d_status + t; a.count = c->d_counts + t; a.cands = c->d_cands + size_t(t) * c->base.capacity;
+            launch_plain(a, s, ev + 5 * t);
+        }
+    }
+    if ((st = c->cuda(cudaGetLastError(), "kernel launch"))) return st;
+    double submit_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - submit0).count();
+    bool timed_out = false;
+    cudaEvent_t done = c->fused ? ev[4] : ev[5 * (count - 1) + 4];
+    cudaError_t e = wait_event(done, kWaitSeconds, &timed_out);
+    if (timed_out) return c->fail(BRP_E_TIMEOUT, "GPU run exceeded its deadline");
+    if ((st = c->cuda(e, "GPU run"))) return st;
+    brp_timings t{};
+    t.submit_ms = submit_ms;
+    for (int k = 0; k < 4; ++k) c->last_stage_ms[k] = 0;
+    const uint32_t groups = c->fused ? 1 : count;
+    for (uint32_t g = 0; g < groups; ++g)
+        for (int k = 0; k < 4; ++k) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[5 * g + k], ev[5 * g + k + 1]);
+            t.stage_ms[k] += ms;
+            c->last_stage_ms[k] += ms;
+            if (template_stage_ms) {
+                if (c->fused) for (uint32_t r = 0; r < count; ++r) template_stage_ms[4 * r + k] = ms / count;
+                else template_stage_ms[4 * g + k] = ms;
+            }
+        }
+    c->last_count = count;
+    t.cpu_ms = cpu_ms_now() - cpu0;
+    t.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
+    if (timings) *timings = t;
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_snapshot(brp_ctx* c, float* resampled, float* fft, float* power, float* summed) {
+    if (!c) return set_thread_error(BRP_E_ARGUMENT, "null context");
+    if (!c->last_count) return c->fail(BRP_E_RUNTIME, "snapshot before run");
+    int st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    const uint32_t g = c->last_count - 1;
+    const brp_params& p = c->templates[g];
+    const uint32_t slot = c->fused ? g : 0;
+    if (resampled) {
+        float mean = 0;
+        if ((st = c->cuda(cudaMemcpy(resampled, c->d_raw, size_t(p.steps) * 4, cudaMemcpyDeviceToHost), "snapshot")) ||
+            (st = c->cuda(cudaMemcpy(&mean, c->d_mean + (c->fused ? g : 0), 4, cudaMemcpyDeviceToHost), "snapshot")))
+            return st;
+        std::fill(resampled + p.steps, resampled + p.n, mean);
+    }
+    if (fft && (st = c->cuda(cudaMemcpy(fft, c->d_fft, (size_t(c->lp.M) + 1) * 8, cudaMemcpyDeviceToHost), "snapshot")))
+        return st;
+    if (power && (st = c->cuda(cudaMemcpy(power, c->d_power + size_t(slot) * c->lp.M, size_t(c->lp.M) * 4,
+                                          cudaMemcpyDeviceToHost), "snapshot")))
+        return st;
+    if (summed && (st = c->cuda(cudaMemcpy(summed, c->d_summed, size_t(5) * p.fundamental * 4, cudaMemcpyDeviceToHost),
+                                "snapshot")))
+        return st;
+    return BRP_OK;
+}
+
+static void sort_candidates(brp_candidate* c, size_t n) {
+    std::sort(c, c + n, [](const brp_candidate& a, const brp_candidate& b) {
+        return a.level != b.level ? a.level < b.level : a.bin < b.bin;
+    });
+}
+
+extern "C" int brp_cuda_candidates(brp_ctx* c, uint32_t slot, brp_candidate* out, uint32_t cap, uint32_t* count) {
+    if (!c || !count) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (slot == UINT32_MAX) slot = c->last_count ? c->last_count - 1 : 0;
+    if (slot >= c->last_count) return c->fail(BRP_E_RUNTIME, "candidate slot outside executed batch");
+    int st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    uint32_t hdr[2];
+    if ((st = c->cuda(cudaMemcpy(&hdr[0], c->d_counts + slot, 4, cudaMemcpyDeviceToHost), "candidates")) ||
+        (st = c->cuda(cudaMemcpy(&hdr[1], c->d_status + slot, 4, cudaMemcpyDeviceToHost), "candidates")))
+        return st;
+    *count = hdr[0];
+    if (hdr[1] || hdr[0] > c->base.capacity)
+        return c->fail(BRP_E_RESULT, "GPU invalid resample index or candidate overflow; no valid result");
+    std::vector<brp_candidate> tmp(hdr[0]);
+    if (hdr[0] && (st = c->cuda(cudaMemcpy(tmp.data(), c->d_cands + size_t(slot) * c->base.capacity,
+                                           size_t(hdr[0]) * sizeof(brp_candidate), cudaMemcpyDeviceToHost),
+                                "candidates")))
+        return st;
+    sort_candidates(tmp.data(), tmp.size());
+    if (out) std::memcpy(out, tmp.data(), std::min<size_t>(cap, tmp.size()) * sizeof(brp_candidate));
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_device_info(brp_ctx* c, char* buffer, size_t length) {
+    if (!c || !buffer || !length) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    cudaDeviceProp prop{};
+    int st;
+    if ((st = c->cuda(cudaGetDeviceProperties(&prop, c->device), "cudaGetDeviceProperties"))) return st;
+    int rt = 0, drv = 0;
+    cudaRuntimeGetVersion(&rt);
+    cudaDriverGetVersion(&drv);
+    snprintf(buffer, length,
+             "%s; CUDA sm_%d%d; SMs=%d; runtime=%d; driver=%d; shared_per_block_optin=%zu; L2=%d; pipeline=%s; "
+             "decomposition=%ux%u",
+             prop.name, prop.major, prop.minor, prop.multiProcessorCount, rt, drv, prop.sharedMemPerBlockOptin,
+             prop.l2CacheSize, c->fused ? "fused" : "plain", c->lp.L1, c->lp.L2);
+    return BRP_OK;
+}
+
+extern "C" uint64_t brp_cuda_allocated_bytes(const brp_ctx* c) { return c ? c->allocated : 0; }
+
+extern "C" int brp_cuda_profile_counters(brp_ctx* c, char* buffer, size_t length) {
+    if (!c || !buffer || !length) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    snprintf(buffer, length,
+             "{\"source\": \"cuda events\", \"templates\": %u, \"stage_ms\": {\"resample\": %.6f, \"fft\": %.6f, "
+             "\"power\": %.6f, \"harmonic_candidate\": %.6f}}",
+             c->last_count, c->last_stage_ms[0], c->last_stage_ms[1], c->last_stage_ms[2], c->last_stage_ms[3]);
+    return BRP_OK;
+}
+
+// ===================================================================== bank
+struct brp_bank {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<uint32_t> n, unpadded;
+    std::vector<float*> d_series;
+    std::map<uint32_t, LengthPlan> plans;  // by n
+    struct ClassBuffers { float2* work = nullptr; float* power = nullptr; double* partial = nullptr; uint32_t group = 0; };
+    std::map<uint32_t, ClassBuffers> classes;
+    uint32_t max_templates = 0, capacity = 0;
+    std::vector<void*> allocations;
+    brp_params* d_params = nullptr;
+    const float** d_inputs = nullptr;
+    uint32_t *d_counts = nullptr, *d_status = nullptr;
+    float* d_mean = nullptr;
+    brp_candidate* d_cands = nullptr;
+    brp_candidate* d_compact = nullptr;
+    uint64_t* d_offsets = nullptr;
+    uint64_t compact_cap = 0;
+    brp_params* h_params = nullptr;
+    const float** h_inputs = nullptr;
+    uint32_t* h_counts = nullptr;
+    uint64_t* h_offsets = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> graph_key;
+    uint32_t kernels_per_run = 0;
+    cudaEvent_t done = nullptr;
+    std::string error;
+
+    int fail(int code, const std::string& msg) {
+        error = msg;
+        g_thread_error = msg;
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return BRP_OK;
+        return fail(BRP_E_RUNTIME, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    template <class T>
+    int alloc(T** p, size_t count, const char* what) {
+        if (cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess)
+            return fail(BRP_E_RUNTIME, std::string("cudaMalloc failed: ") + what);
+        allocations.push_back(*p);
+        return BRP_OK;
+    }
+    ~brp_bank() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (done) cudaEventDestroy(done);
+        for (auto p : allocations) cudaFree(p);
+        for (auto& kv : plans) free_length_plan(kv.second);
+        if (h_params) cudaFreeHost(h_params);
+        if (h_inputs) cudaFreeHost(h_inputs);
+        if (h_counts) cudaFreeHost(h_counts);
+        if (h_offsets) cudaFreeHost(h_offsets);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" const char* brp_cuda_bank_last_error(const brp_bank* b) { return b ? b->error.c_str() : g_thread_error.c_str(); }
+
+// Templates of one length class run in groups of `group` templates per launch;
+// the class's intermediate buffers hold one group.
+static uint32_t default_group(uint32_t n) {
+    // About 24 MiB of intermediates per template at n = 2^22; groups of 8
+    // keep a group's working set near the 126 MB L2.
+    if (n >= (1u << 22)) return 8;
+    if (n >= (1u << 20)) return 16;
+    return 32;
+}
+
+extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, const uint32_t* unpadded,
+                                    uint32_t max_templates, uint32_t capacity, int32_t device, brp_bank** out) {
+    if (!n || !unpadded || !out || !series_count || !max_templates || !capacity)
+        return set_thread_error(BRP_E_ARGUMENT, "invalid bank arguments");
+    *out = nullptr;
+    auto* b = new (std::nothrow) brp_bank;
+    if (!b) return set_thread_error(BRP_E_RUNTIME, "out of host memory");
+    auto cleanup = [&](int code) { std::string m = b->error; delete b; return set_thread_error(code, m); };
+    b->device = device;
+    if (b->device < 0) cudaGetDevice(&b->device);
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return cleanup(st);
+    if ((st = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) return cleanup(st);
+    if ((st = b->cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "cudaEventCreate"))) return cleanup(st);
+    b->n.assign(n, n + series_count);
+    b->unpadded.assign(unpadded, unpadded + series_count);
+    b->max_templates = max_templates;
+    b->capacity = capacity;
+    for (uint32_t s = 0; s < series_count; ++s) {
+        if (unpadded[s] < 2 || unpadded[s] > n[s]) return b->fail(BRP_E_ARGUMENT, "invalid series length"), cleanup(BRP_E_ARGUMENT);
+        float* d = nullptr;
+        if ((st = b->alloc(&d, unpadded[s], "series"))) return cleanup(st);
+        b->d_series.push_back(d);
+        if (!b->plans.count(n[s])) {
+            std::string e = make_length_plan(n[s], b->plans[n[s]], b->stream);
+            if (!e.empty()) { b->fail(BRP_E_ARGUMENT, e); return cleanup(BRP_E_ARGUMENT); }
+            if (!b->plans[n[s]].fused) { b->fail(BRP_E_ARGUMENT, "bank search needs n >= 8192"); return cleanup(BRP_E_ARGUMENT); }
+        }
+    }
+    for (auto& kv : b->plans) {
+        const LengthPlan& lp = kv.second;
+        brp_bank::ClassBuffers cb;
+        cb.group = std::min(default_group(lp.n), max_templates);
+        if ((st = b->alloc(&cb.work, size_t(cb.group) * lp.M, "work")) ||
+            (st = b->alloc(&cb.power, size_t(cb.group) * lp.M, "power")) ||
+            (st = b->alloc(&cb.partial, size_t(cb.group) * lp.blocks1(), "partial")))
+            return cleanup(st);
+        b->classes[kv.first] = cb;
+    }
+    b->compact_cap = uint64_t(max_templates) * capacity;
+    if ((st = b->alloc(&b->d_params, max_templates, "params")) || (st = b->alloc(&b->d_inputs, max_templates, "inputs")) ||
+        (st = b->alloc(&b->d_counts, max_templates, "counts")) || (st = b->alloc(&b->d_status, max_templates, "status")) ||
+        (st = b->alloc(&b->d_mean, max_templates, "mean")) ||
+        (st = b->alloc(&b->d_cands, size_t(max_templates) * capacity, "candidates")) ||
+        (st = b->alloc(&b->d_compact, b->compact_cap, "compact")) ||
+        (st = b->alloc(&b->d_offsets, size_t(max_templates) + 1, "offsets")))
+        return cleanup(st);
+    if ((st = b->cuda(cudaMallocHost(&b->h_params, max_templates * sizeof(brp_params)), "cudaMallocHost")) ||
+        (st = b->cuda(cudaMallocHost(&b->h_inputs, max_templates * sizeof(void*)), "cudaMallocHost")) ||
+        (st = b->cuda(cudaMallocHost(&b->h_counts, 2 * max_templates * sizeof(uint32_t)), "cudaMallocHost")) ||
+        (st = b->cuda(cudaMallocHost(&b->h_offsets, (max_templates + 1) * sizeof(uint64_t)), "cudaMallocHost")))
+        return cleanup(st);
+    *out = b;
+    return BRP_OK;
+}
+
+extern "C" void brp_cuda_bank_destroy(brp_bank* b) { delete b; }
+
+extern "C" int brp_cuda_bank_set_series(brp_bank* b, uint32_t s, const float* input) {
+    if (!b || !input) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (s >= b->d_series.size()) return b->fail(BRP_E_ARGUMENT, "series index out of range");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    return b->cuda(cudaMemcpyAsync(b->d_series[s], input, size_t(b->unpadded[s]) * 4, cudaMemcpyHostToDevice, b->stream),
+                   "series upload");
+}
+
+// Records the whole bank search on b->stream (captured into the graph).
+static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, const std::vector<uint32_t>& spans,
+                        uint32_t count) {
+    cudaStream_t s = b->stream;
+    cudaMemsetAsync(b->d_counts, 0, count * sizeof(uint32_t), s);
+    cudaMemsetAsync(b->d_status, 0, count * sizeof(uint32_t), s);
+    uint32_t kernels = 0;
+    uint32_t t = 0;
+    while (t < count) {
+        const uint32_t n = sorted_n[t];
+        const LengthPlan& lp = b->plans.at(n);
+        const brp_bank::ClassBuffers& cb = b->classes.at(n);
+        uint32_t end = t;
+        while (end < count && sorted_n[end] == n && end - t < cb.group) ++end;
+        const uint32_t g = end - t;
+        FusedArgs a{};
+        a.inputs = b->d_inputs + t;
+        a.params = b->d_params + t;
+        a.n = lp.n; a.M = lp.M; a.L1 = lp.L1; a.L2 = lp.L2; a.C = lp.C; a.R = lp.R;
+        a.plan1[0] = lp.plan1.count; a.plan2[0] = lp.plan2.count;
+        for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
+        a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
+        a.work = cb.work; a.work_stride = lp.M;
+        a.power = cb.power; a.power_stride = lp.M;
+        a.partial = cb.partial; a.partial_stride = lp.blocks1();
+        a.mean = b->d_mean + t; a.status = b->d_status + t; a.counts = b->d_counts + t;
+        a.cands = b->d_cands + size_t(t) * b->capacity;
+        a.capacity = b->capacity;
+        a.snap = -1;
+        uint32_t span = 0;
+        for (uint32_t u = t; u < end; ++u) span = std::max(span, spans[u]);
+        launch_fused_pass1(a, lp, g, s);
+        launch_fused_pass2(a, lp, g, s);
+        launch_fused_harmonic(a, lp, g, span, s);
+        kernels += 3;
+        t = end;
+    }
+    launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_compact, b->compact_cap, b->d_offsets, s);
+    b->kernels_per_run = kernels + 1;
+}
+
+extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const uint32_t* series_of, uint32_t count,
+                                 brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status) {
+    if (!b || !templates || !series_of || !counts || !status) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (!count || count > b->max_templates) return b->fail(BRP_E_ARGUMENT, "template count outside 1..max_templates");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    // Order templates by length class (stable), remembering the caller's order.
+    std::vector<uint32_t> order(count);
+    for (uint32_t t = 0; t < count; ++t) {
+        order[t] = t;
+        const uint32_t s = series_of[t];
+        if (s >= b->n.size()) return b->fail(BRP_E_ARGUMENT, "series index out of range");
+        const brp_params& p = templates[t];
+        if (p.n != b->n[s] || p.unpadded != b->unpadded[s]) return b->fail(BRP_E_ARGUMENT, "template does not match its series");
+        std::string v = validate_dims(p);
+        if (!v.empty()) return b->fail(BRP_E_ARGUMENT, v);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return b->n[series_of[x]] > b->n[series_of[y]]; });
+    std::vector<uint32_t> sorted_n(count), spans(count);
+    std::vector<uint64_t> key;
+    key.push_back(count);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t t = order[k];
+        b->h_params[k] = templates[t];
+        b->h_params[k].capacity = b->capacity;
+        b->h_inputs[k] = b->d_series[series_of[t]];
+        sorted_n[k] = b->n[series_of[t]];
+        spans[k] = std::max(templates[t].fundamental, templates[t].harmonic + 8);
+        key.push_back((uint64_t(sorted_n[k]) << 32) | spans[k]);
+    }
+    cudaStream_t s = b->stream;
+    if ((st = b->cuda(cudaMemcpyAsync(b->d_params, b->h_params, count * sizeof(brp_params), cudaMemcpyHostToDevice, s),
+                      "params upload")) ||
+        (st = b->cuda(cudaMemcpyAsync(b->d_inputs, b->h_inputs, count * sizeof(void*), cudaMemcpyHostToDevice, s),
+                      "inputs upload")))
+        return st;
+    if (key != b->graph_key || !b->exec) {
+        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+        if ((st = b->cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture"))) return st;
+        record_bank(b, sorted_n, spans, count);
+        cudaError_t e = cudaStreamEndCapture(s, &b->graph);
+        if ((st = b->cuda(e, "end capture"))) return st;
+        if ((st = b->cuda(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate"))) return st;
+        b->graph_key = key;
+    }
+    if ((st = b->cuda(cudaGraphLaunch(b->exec, s), "graph launch"))) return st;
+    uint32_t* h_status = b->h_counts + b->max_templates;
+    cudaMemcpyAsync(b->h_counts, b->d_counts, count * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_status, b->d_status, count * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(b->h_offsets, b->d_offsets, (count + 1) * 8, cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(b->done, s);
+    bool timed_out = false;
+    cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
+    if (timed_out) return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
+    if ((st = b->cuda(e, "bank search"))) return st;
+    const uint64_t total = b->h_offsets[count];
+    std::vector<brp_candidate> compact(total);
+    if (total && (st = b->cuda(cudaMemcpy(compact.data(), b->d_compact, total * sizeof(brp_candidate),
+                                          cudaMemcpyDeviceToHost), "candidates download")))
+        return st;
+    // Back to the caller's order, candidates sorted by (level, bin) per template.
+    std::vector<uint64_t> dst_off(count + 1, 0);
+    std::vector<uint32_t> kept(count);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t t = order[k];
+        counts[t] = b->h_counts[k];
+        status[t] = h_status[k] | (b->h_counts[k] > b->capacity ? BRP_STATUS_OVERFLOW : 0u);
+        kept[t] = uint32_t(b->h_offsets[k + 1] - b->h_offsets[k]);
+    }
+    for (uint32_t t = 0; t < count; ++t) dst_off[t + 1] = dst_off[t] + kept[t];
+    bool bad = false;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t t = order[k];
+        if (status[t]) bad = true;
+        if (dst_off[t] + kept[t] > out_cap) { bad = true; continue; }
+        if (out) {
+            std::memcpy(out + dst_off[t], compact.data() + b->h_offsets[k], size_t(kept[t]) * sizeof(brp_candidate));
+            sort_candidates(out + dst_off[t], kept[t]);
+        }
+    }
+    if (dst_off[count] > out_cap) return b->fail(BRP_E_RESULT, "candidate output buffer too small");
+    if (bad) return b->fail(BRP_E_RESULT, "GPU invalid resample index or candidate overflow; no valid result");
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_bank_launch(brp_bank* b) {
+    if (!b || !b->exec) return set_thread_error(BRP_E_ARGUMENT, "no captured bank graph");
+    return b->cuda(cudaGraphLaunch(b->exec, b->stream), "graph launch");
+}
+
+extern "C" void* brp_cuda_bank_stream(brp_bank* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+extern "C" uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* b) { return b ? b->kernels_per_run : 0; }

@@ -1,0 +1,105 @@
+// Internal interfaces of the CUDA backend: length plans, kernel argument
+// blocks and kernel launchers.  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "../../include/brp_cuda.h"
+
+namespace brp {
+
+// Radix plan of one shared-memory FFT (mirrors the device struct in fft_device.cuh).
+struct RadixPlanHost {
+    int count = 0;
+    int radix[6] = {0, 0, 0, 0, 0, 0};
+};
+RadixPlanHost radix_plan(uint32_t length);
+
+// Tables of one FFT length class, all FP64-generated and rounded once to FP32.
+//   tw1[L1], tw2[L2]       : W_L^e for the two shared-memory passes
+//   fs_hi/fs_lo (split 2^11): W_M^e, e < M (four-step twiddles)
+//   rl_hi/rl_lo (split 2^11): W_N^e, e < N (real post-process and padding term)
+//   twb[B]                  : W_B^e, B = M or M/3 (global passes of the plain pipeline)
+struct LengthPlan {
+    uint32_t n = 0, M = 0;     // series length and packed complex length M = n/2
+    uint32_t radix = 1, B = 0; // M = radix * B (radix 1 or 3), for the plain pipeline
+    bool fused = false;        // fused two-pass pipeline available for this length
+    uint32_t L1 = 0, L2 = 0;   // M = L1 * L2; pass 1 transforms columns of L1, pass 2 rows of L2
+    uint32_t C = 0;            // pass 1: columns per CTA
+    uint32_t R = 0;            // pass 2: row pairs per CTA
+    uint32_t maxe = 16;        // elements per thread held during a shared-memory pass
+    uint32_t harm_tile = 2048; // harmonic kernel: trial bins per CTA
+    RadixPlanHost plan1, plan2, planB;
+    float2* d_tables = nullptr;
+    size_t tables_bytes = 0;
+    const float2 *tw1 = nullptr, *tw2 = nullptr, *fs_hi = nullptr, *fs_lo = nullptr, *rl_hi = nullptr,
+                 *rl_lo = nullptr, *twb = nullptr;
+    uint32_t blocks1() const { return L2 / C; }        // pass-1 CTAs per template
+    uint32_t blocks2() const { return L1 / (2 * R); }  // pass-2 CTAs per template
+    size_t smem1() const;
+    size_t smem2() const;
+};
+// Chooses the decomposition for length n and uploads its tables.  Returns an
+// error message or empty.
+std::string make_length_plan(uint32_t n, LengthPlan& plan, cudaStream_t stream);
+void free_length_plan(LengthPlan& plan);
+
+constexpr uint32_t kSplitLog2 = 11;
+
+// Device views passed to the fused kernels.  Per-template arrays are indexed
+// by blockIdx.y (the template within the launch).
+struct FusedArgs {
+    const float* const* inputs;  // per template: series (unpadded floats)
+    const brp_params* params;    // per template
+    uint32_t n, M, L1, L2, C, R;
+    int plan1[7], plan2[7];      // count followed by radices
+    const float2 *tw1, *tw2, *fs_hi, *fs_lo, *rl_hi, *rl_lo;
+    float2* work;     // per template: M complex (four-step intermediate)
+    size_t work_stride;
+    float* power;     // per template: M floats (P[k] = |X_k|^2 / n, P[0] = 0)
+    size_t power_stride;
+    double* partial;  // per template: blocks1 partial sums of the resampled series
+    uint32_t partial_stride;
+    float* mean;      // per template: padding value (written by pass 2)
+    uint32_t* status; // per template: BRP_STATUS_* bits
+    uint32_t* counts; // per template: candidate count
+    brp_candidate* cands;  // per template: capacity candidates
+    uint32_t capacity;
+    // Snapshot outputs, written for template `snap` of the launch only (-1: none).
+    int snap;
+    float* snap_raw;     // resampled series (first steps values)
+    float2* snap_fft;    // X[0..M]
+    float* snap_summed;  // 5*fundamental
+};
+
+cudaError_t set_fused_attributes(size_t max_dynamic_smem);
+void launch_fused_pass1(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s);
+void launch_fused_pass2(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s);
+void launch_fused_harmonic(const FusedArgs& a, const LengthPlan& lp, uint32_t count, uint32_t max_span,
+                           cudaStream_t s);
+
+// Step-by-step pipeline (one template; buffers sized for the length class).
+struct PlainArgs {
+    const float* input;
+    brp_params p;
+    const LengthPlan* lp;
+    float* raw;       // steps floats
+    double* partial;  // ceil(steps/256) partial sums
+    float* mean;      // 1 float
+    float2* a;        // M complex
+    float2* b;        // M complex
+    float2* fft;      // M+1 complex (X)
+    float* power;     // M floats
+    float* summed;    // 5*fundamental floats
+    uint32_t* status; // 1 word
+    uint32_t* count;  // 1 word
+    brp_candidate* cands;
+};
+// Records the plain pipeline on stream s; ev (optional, 5 events) brackets the 4 stages.
+void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev);
+
+void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
+                         brp_candidate* out, uint64_t out_cap, uint64_t* offsets, cudaStream_t s);
+
+}  // namespace brp

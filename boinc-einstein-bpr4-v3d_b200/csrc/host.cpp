@@ -1,0 +1,203 @@
+// Host-side code around the search path: template constants, the chi-square
+// thresholds and the bank-wide toplist.  These restate the reference's host
+// functions (src/science.cpp:41-65, src/workload.cpp:108-159) so that a bank
+// search through this library produces the reference's thresholds, candidate
+// filtering and final ranking.  Compiled with -ffp-contract=off: the FP32
+// expressions round exactly where the reference's do.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include "../../include/brp_cuda.h"
+#include "resample_math.h"
+
+namespace {
+thread_local std::string g_host_error;
+int host_fail(const char* msg) { g_host_error = msg; return BRP_E_ARGUMENT; }
+const uint32_t k_lut[130] = BRP_LUT_BITS;
+bool single_bit(uint32_t x) { return x && !(x & (x - 1)); }
+
+brp_resample_consts consts_of(const brp_params& p) {
+    brp_resample_consts c;
+    c.tau = p.tau; c.omega = p.omega; c.psi = p.psi; c.dt = p.dt; c.step_inv = p.step_inv; c.s0 = p.s0;
+    c.flags = p.flags;
+    return c;
+}
+}  // namespace
+
+const char* brp_host_last_error() { return g_host_error.c_str(); }
+
+extern "C" int brp_host_resampling_steps(brp_params* p) {
+    // src/science.cpp:41-45: the largest steps with steps - offset(steps) < unpadded - 1.
+    if (!p || p->unpadded < 2) return host_fail("invalid template");
+    const brp_resample_consts c = consts_of(*p);
+    p->steps = p->unpadded - 1;
+    while (p->steps && float(p->steps) - brp_sample_offset(p->steps, c, k_lut) >= float(p->unpadded - 1)) --p->steps;
+    if (!p->steps) return host_fail("template produces empty series");
+    return BRP_OK;
+}
+
+extern "C" int brp_host_parameters(uint32_t n, uint32_t unpadded, float tau, float period, float psi, float dt,
+                                   brp_params* out) {
+    // src/science.cpp:46-65.
+    if (!out) return host_fail("null output");
+    uint32_t radix = single_bit(n) ? 1 : ((n % 3 == 0 && single_bit(n / 3)) ? 3 : 0);
+    if (!radix || n < 64 || n > 3 * (1u << 22) || unpadded < 32 || unpadded > n || dt <= 0 || period <= 0 || tau < 0 ||
+        !std::isfinite(tau + period + psi + dt))
+        return host_fail("invalid observation/template");
+    brp_params p;
+    std::memset(&p, 0, sizeof p);
+    p.n = n; p.unpadded = unpadded; p.fft_n = n; p.fft_radix = radix; p.fft_base = n / radix;
+    p.logn = uint32_t(__builtin_ctz(p.fft_base));
+    p.tau = tau;
+    p.omega = float(2.0 * M_PI / double(period));
+    p.psi = psi; p.dt = dt; p.step_inv = 1.0f / dt;
+    p.s0 = float(double(tau) * std::sin(double(psi)) * double(p.step_inv));
+    if (!std::isfinite(p.omega) || !std::isfinite(p.step_inv) || !std::isfinite(p.s0) ||
+        !std::isfinite(p.tau * p.step_inv) || !std::isfinite(float(unpadded) * p.dt) ||
+        !std::isfinite(p.omega * (float(unpadded) * p.dt) + p.psi))
+        return host_fail("template exceeds finite FP32 arithmetic domain");
+    int st = brp_host_resampling_steps(&p);
+    if (st) return st;
+    p.harmonic = n / 2; p.fundamental = n / 2; p.window = 8;
+    const float thresholds[5] = {20, 30, 45, 70, 110};
+    std::memcpy(p.threshold, thresholds, sizeof thresholds);
+    p.capacity = 65536;
+    *out = p;
+    return BRP_OK;
+}
+
+// Chi-square upper tail Q(x; nu) for even nu = 2k: exp(-x/2) sum_{i<k} (x/2)^i / i!.
+// Closed form of the regularized incomplete gamma function at integer order,
+// standing in for gsl_cdf_chisq_Q (src/workload.cpp:146).
+static double chisq_Q(double x, double nu) {
+    if (!(x >= 0) || nu < 2 || std::fmod(nu, 2.0) != 0) return NAN;
+    double y = 0.5 * x;
+    int k = int(nu / 2);
+    if (y <= 600) {
+        double term = 1, sum = 1;
+        for (int i = 1; i < k; ++i) { term *= y / i; sum += term; }
+        return std::exp(-y) * sum;
+    }
+    double ly = std::log(y), m = (k - 1) * ly - std::lgamma(double(k)), acc = 0;
+    for (int i = 0; i < k; ++i) acc += std::exp(i * ly - std::lgamma(double(i) + 1) - m);
+    return std::exp(-y + m + std::log(acc));
+}
+
+// Inverse of chisq_Q in x by safeguarded Newton iteration on log Q, standing in
+// for gsl_cdf_chisq_Qinv (src/workload.cpp:122).
+static double chisq_Qinv(double q, double nu) {
+    if (!(q > 0 && q < 1) || nu < 2 || std::fmod(nu, 2.0) != 0) return NAN;
+    double lo = 0, hi = nu + 10;
+    while (chisq_Q(hi, nu) > q) { lo = hi; hi *= 2; }
+    double x = 0.5 * (lo + hi), lq = std::log(q);
+    int k = int(nu / 2);
+    for (int it = 0; it < 200; ++it) {
+        double Q = chisq_Q(x, nu);
+        if (Q > q) lo = x; else hi = x;
+        double lpdf = (k - 1) * std::log(0.5 * x) - 0.5 * x - std::log(2.0) - std::lgamma(double(k));
+        double next = x + (std::log(Q) - lq) / std::exp(lpdf - std::log(Q));
+        if (!(next > lo && next < hi)) next = 0.5 * (lo + hi);
+        if (std::fabs(next - x) <= 1e-16 * x || hi - lo <= 4e-16 * x) { x = next; break; }
+        x = next;
+    }
+    return x;
+}
+
+extern "C" double brp_host_chisq_Q(double x, double nu) { return chisq_Q(x, nu); }
+extern "C" double brp_host_chisq_Qinv(double q, double nu) { return chisq_Qinv(q, nu); }
+
+extern "C" int brp_host_search_parameters(uint32_t n, uint32_t samples, double sample_us, double period, double tau,
+                                          double psi, double f0, double false_alarm, uint32_t window,
+                                          brp_params* out) {
+    // src/workload.cpp:108-125.
+    if (!out) return host_fail("null output");
+    if (!std::isfinite(f0 + false_alarm) || f0 <= 0 || false_alarm <= 0 || false_alarm >= 1 || !window)
+        return host_fail("invalid search parameters");
+    brp_params p;
+    int st = brp_host_parameters(n, samples, float(tau), float(period), float(psi), float(sample_us * 1e-6), &p);
+    if (st) return st;
+    p.flags = 2 | 4;  // production FMA arithmetic
+    p.s0 = (p.tau * std::sin(p.psi)) * p.step_inv;
+    st = brp_host_resampling_steps(&p);
+    if (st) return st;
+    double seconds = n * sample_us * 1e-6;
+    p.window = uint32_t(window * 0.5 + 0.5);
+    if (p.window >= p.n / 2 + 1) return host_fail("search window exceeds spectrum");
+    double limit = p.n / 2 + 1 - p.window;
+    p.fundamental = uint32_t(std::min(limit, f0 * seconds + 0.5));
+    p.harmonic = uint32_t(std::min(limit, 16 * f0 * seconds + 0.5));
+    float probability = 1.0 - std::pow(1.0 - false_alarm, 1.0 / (p.n / 2 + 1));
+    if (!(probability > 0 && probability < 1)) return host_fail("false-alarm probability outside representable domain");
+    for (uint32_t h = 0; h < 5; ++h) p.threshold[h] = 0.5 * chisq_Qinv(probability, 2.0 * (1u << h));
+    if (p.fundamental <= p.window) return host_fail("empty frequency search");
+    *out = p;
+    return BRP_OK;
+}
+
+// ---- bank-wide toplist: 5 harmonic levels x 100 rows (src/workload.cpp:126-159) ----
+struct brp_toplist { brp_bank_candidate rows[500]; };
+
+extern "C" brp_toplist* brp_toplist_create(void) {
+    auto* t = new (std::nothrow) brp_toplist;
+    if (t) std::memset(t, 0, sizeof *t);
+    return t;
+}
+extern "C" void brp_toplist_destroy(brp_toplist* t) { delete t; }
+
+extern "C" void brp_toplist_thresholds(const brp_toplist* t, brp_params* p) {
+    for (uint32_t h = 0; h < 5; ++h) p->threshold[h] = std::max(p->threshold[h], float(t->rows[(h + 1) * 100 - 1].power));
+}
+
+// The reference sorts with the C library's qsort and these comparators; equal
+// keys keep whatever order that qsort gives, so the same call is made here.
+static int by_power(const void* x, const void* y) {
+    auto a = static_cast<const brp_bank_candidate*>(x), b = static_cast<const brp_bank_candidate*>(y);
+    return a->power < b->power ? 1 : (a->power > b->power ? -1 : 0);
+}
+static int by_significance(const void* x, const void* y) {
+    auto a = static_cast<const brp_bank_candidate*>(x), b = static_cast<const brp_bank_candidate*>(y);
+    return a->significance < b->significance ? 1 : (a->significance > b->significance ? -1 : 0);
+}
+
+extern "C" int brp_toplist_retain(brp_toplist* t, const brp_candidate* cands, uint32_t count, double period,
+                                  double tau, double psi, const brp_params* p) {
+    for (uint32_t k = 0; k < count; ++k) {
+        const brp_candidate c = cands[k];
+        if (c.level >= 5 || c.bin < p->window || c.bin >= p->fundamental || !std::isfinite(c.power))
+            return host_fail("invalid compact candidate");
+        uint32_t first = c.level * 100, last = first + 99;
+        if (c.power <= p->threshold[c.level] || c.power <= t->rows[last].power) continue;
+        int place = int(last);
+        for (uint32_t i = first; i <= last; ++i)
+            if (t->rows[i].bin == c.bin) { place = t->rows[i].power < c.power ? int(i) : -1; break; }
+        if (place >= int(first)) {
+            t->rows[place] = {c.power, float(period), float(tau), float(psi), 0, 1u << c.level, c.bin};
+            std::qsort(t->rows + first, 100, sizeof(brp_bank_candidate), by_power);
+        }
+    }
+    return BRP_OK;
+}
+
+extern "C" uint32_t brp_toplist_final(const brp_toplist* t, brp_bank_candidate* out) {
+    brp_bank_candidate copy[500];
+    std::memcpy(copy, t->rows, sizeof copy);
+    for (auto& c : copy) {
+        if (!c.harmonics) { c.significance = -10; continue; }
+        double probability = chisq_Q(2 * c.power, 2.0 * c.harmonics);
+        c.significance = probability > 0 ? -std::log10(probability) : 320;
+        c.power /= float(std::sqrt(float(c.harmonics)));
+    }
+    std::qsort(copy, 500, sizeof(brp_bank_candidate), by_significance);
+    uint32_t count = 0;
+    while (count < 100 && copy[0].significance > 0) {
+        out[count++] = copy[0];
+        uint32_t bin = copy[0].bin;
+        for (auto& c : copy) if (c.bin == bin) c.significance = -10;
+        std::qsort(copy, 500, sizeof(brp_bank_candidate), by_significance);
+    }
+    return count;
+}

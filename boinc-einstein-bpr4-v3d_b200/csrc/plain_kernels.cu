@@ -1,0 +1,251 @@
+// Step-by-step per-template pipeline: one kernel per stage with global-memory
+// FFT passes, the structure of the reference's recorded command sequence
+// (src/vulkan.cpp:226-262): resample, mean, prepare, radix-8/4/2 Stockham
+// passes, radix-3 combination, real post-process + power, harmonic summing
+// with compaction.  It is the per-template comparator of the fused pipeline
+// and a second, independent GPU implementation for cross-checks.
+#include "brp_internal.h"
+#include "fft_device.cuh"
+#include "resample_math.h"
+
+namespace brp {
+
+__constant__ uint32_t c_plain_lut_bits[130] = BRP_LUT_BITS;
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__global__ void __launch_bounds__(kBlock) plain_resample(const float* __restrict__ in, brp_params p, float* raw,
+                                                         double* partial, uint32_t* status) {
+    __shared__ double red[kBlock / 32];
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    float v = 0.f;
+    if (i < p.steps) {
+        brp_resample_consts rc;
+        rc.tau = p.tau; rc.omega = p.omega; rc.psi = p.psi; rc.dt = p.dt; rc.step_inv = p.step_inv; rc.s0 = p.s0;
+        rc.flags = p.flags;
+        int j = (p.flags & BRP_FLAG_INDEX_FP64) ? brp_resample_index_fp64(i, rc)
+                                                : brp_resample_index(i, rc, c_plain_lut_bits);
+        if (j < 0 || uint32_t(j) >= p.unpadded) atomicOr(status, BRP_STATUS_RESAMPLE_OOB);
+        else v = __ldg(in + j);
+        raw[i] = v;
+    }
+    double s = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < kBlock / 32 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(1024) plain_mean(const double* partial, uint32_t blocks, uint32_t steps,
+                                                   float* mean) {
+    __shared__ double red[32];
+    double s = 0;
+    for (uint32_t i = threadIdx.x; i < blocks; i += 1024) s += partial[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) *mean = float(s / double(steps));
+    }
+}
+
+// Packed complex input z[s] = r[2s] + i r[2s+1] with r[i] = raw[i] (i < steps)
+// or the mean; for M = 3B the three decimated sub-series z[3j + b] go to
+// block b (prepare.comp's source = j*radix + block).
+__global__ void plain_prepare(const float* __restrict__ raw, const float* __restrict__ mean, float2* a, uint32_t steps,
+                              uint32_t M, uint32_t radix, uint32_t B) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    const uint32_t blk = t / B, j = t - blk * B;
+    const uint32_t s = j * radix + blk;
+    const float m = *mean;
+    const uint32_t i0 = 2 * s, i1 = 2 * s + 1;
+    a[t] = make_float2(i0 < steps ? raw[i0] : m, i1 < steps ? raw[i1] : m);
+}
+
+// One global Stockham pass of radix R over `seqs` sequences of length B.
+template <int R>
+__global__ void plain_fft_pass(const float2* __restrict__ in, float2* __restrict__ out, uint32_t B, uint32_t seqs,
+                               uint32_t Ns, const float2* __restrict__ tw) {
+    const uint32_t nbf = B / R;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nbf * seqs) return;
+    const uint32_t sq = t / nbf, j = t - sq * nbf;
+    const uint32_t k = j % Ns, tstep = B / (Ns * R);
+    const float2* src = in + size_t(sq) * B;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * nbf];
+    if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + size_t(r) * k * tstep));
+    }
+    dft<R>(v);
+    float2* dst = out + size_t(sq) * B;
+    const uint32_t base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+}
+
+// Radix-3 combination of three transformed blocks: X[k + m B] =
+// sum_b W_M^{b k} W_3^{b m} A_b[k].
+__global__ void plain_radix3(const float2* __restrict__ in, float2* __restrict__ out, uint32_t B,
+                             const float2* __restrict__ hi, const float2* __restrict__ lo) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B) return;
+    float2 v[3];
+    v[0] = in[k];
+    v[1] = cmul(in[k + B], twiddle2(hi, lo, kSplitLog2, k));
+    v[2] = cmul(in[k + 2 * B], twiddle2(hi, lo, kSplitLog2, 2 * k));
+    dft3(v);
+    out[k] = v[0];
+    out[k + B] = v[1];
+    out[k + 2 * B] = v[2];
+}
+
+// Real post-process (fft_real.comp's formula) and power (power.comp):
+// X_k = 1/2 [(Z_k + Z*_{M-k}) - i W_N^k (Z_k - Z*_{M-k})], k = 0..M;
+// P_k = |X_k|^2 / n for 1 <= k < M, P_0 = 0.
+__global__ void plain_realpost(const float2* __restrict__ Z, float2* fft, float* power, uint32_t M, uint32_t n,
+                               const float2* __restrict__ hi, const float2* __restrict__ lo) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > M) return;
+    const uint32_t q = k == M ? 0 : k, rev = q == 0 ? 0 : M - q;
+    const float2 x = Z[q], y = Z[rev];
+    const float2 w = twiddle2(hi, lo, kSplitLog2, k);
+    float2 s = make_float2(x.x + y.x, x.y - y.y), d = make_float2(x.x - y.x, x.y + y.y);
+    float2 t = cmul(w, d);
+    float2 X = make_float2(0.5f * (s.x + t.y), 0.5f * (s.y - t.x));
+    fft[k] = X;
+    if (k < M) power[k] = k == 0 ? 0.f : (X.x * X.x + X.y * X.y) / float(n);
+}
+
+// harmonic.comp:14-35 (gather form).  grid.y = level.
+__global__ void plain_harmonic(const float* __restrict__ P, brp_params p, float* summed, uint32_t* count,
+                               brp_candidate* cands, uint32_t* status) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x, h = blockIdx.y;
+    if (j >= p.fundamental) return;
+    float value = 0.f;
+    if (h == 0) value = P[j];
+    else {
+        const int64_t w = int64_t(1) << h;
+        int64_t begin = int64_t(j) * w - w / 2, end = int64_t(j) * w + w / 2;
+        if (begin < int64_t(p.window)) begin = p.window;
+        if (end > int64_t(p.harmonic)) end = p.harmonic;
+        if (begin < end) {
+            float first = 0.f, best = 0.f;
+            for (int64_t ii = begin; ii < end; ++ii) {
+                const uint32_t i = uint32_t(ii);
+                float s = P[i];
+                if (h >= 1) s += P[(i * 8 + 8) >> 4];
+                if (h >= 2) s += P[(i * 12 + 8) >> 4] + P[(i * 4 + 8) >> 4];
+                if (h >= 3) s += P[(i * 14 + 8) >> 4] + P[(i * 10 + 8) >> 4] + P[(i * 6 + 8) >> 4] + P[(i * 2 + 8) >> 4];
+                if (h >= 4)
+                    s += P[(i * 15 + 8) >> 4] + P[(i * 13 + 8) >> 4] + P[(i * 11 + 8) >> 4] + P[(i * 9 + 8) >> 4] +
+                         P[(i * 7 + 8) >> 4] + P[(i * 5 + 8) >> 4] + P[(i * 3 + 8) >> 4] + P[(i + 8) >> 4];
+                if (ii == begin) first = best = s;
+                else if (best < s) best = s;
+            }
+            value = best > p.threshold[h] ? best : first;
+        }
+    }
+    summed[size_t(h) * p.fundamental + j] = value;
+    if (j >= p.window && value > p.threshold[h]) {
+        uint32_t slot = atomicAdd(count, 1u);
+        if (slot < p.capacity) {
+            brp_candidate c;
+            c.bin = j; c.level = h; c.power = value; c.reserved = 0;
+            cands[slot] = c;
+        } else {
+            atomicOr(status, BRP_STATUS_OVERFLOW);
+        }
+    }
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t b) { return uint32_t((n + b - 1) / b); }
+
+}  // namespace
+
+void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+    const LengthPlan& lp = *a.lp;
+    const brp_params& p = a.p;
+    if (ev) cudaEventRecord(ev[0], s);
+    const uint32_t rblocks = blocks_for(p.steps, kBlock);
+    plain_resample<<<rblocks, kBlock, 0, s>>>(a.input, p, a.raw, a.partial, a.status);
+    plain_mean<<<1, 1024, 0, s>>>(a.partial, rblocks, p.steps, a.mean);
+    plain_prepare<<<blocks_for(lp.M, kBlock), kBlock, 0, s>>>(a.raw, a.mean, a.a, p.steps, lp.M, lp.radix, lp.B);
+    if (ev) cudaEventRecord(ev[1], s);
+    // Radix-8 passes while at least three factors of two remain, then 4 or 2.
+    float2 *src = a.a, *dst = a.b;
+    const uint32_t seqs = lp.radix;
+    uint32_t Ns = 1;
+    while (Ns < lp.B) {
+        const uint32_t left = lp.B / Ns;
+        if (left >= 8) {
+            plain_fft_pass<8><<<blocks_for(uint64_t(lp.B / 8) * seqs, kBlock), kBlock, 0, s>>>(src, dst, lp.B, seqs, Ns, lp.twb);
+            Ns *= 8;
+        } else if (left == 4) {
+            plain_fft_pass<4><<<blocks_for(uint64_t(lp.B / 4) * seqs, kBlock), kBlock, 0, s>>>(src, dst, lp.B, seqs, Ns, lp.twb);
+            Ns *= 4;
+        } else {
+            plain_fft_pass<2><<<blocks_for(uint64_t(lp.B / 2) * seqs, kBlock), kBlock, 0, s>>>(src, dst, lp.B, seqs, Ns, lp.twb);
+            Ns *= 2;
+        }
+        float2* t = src; src = dst; dst = t;
+    }
+    if (lp.radix == 3) {
+        plain_radix3<<<blocks_for(lp.B, kBlock), kBlock, 0, s>>>(src, dst, lp.B, lp.fs_hi, lp.fs_lo);
+        float2* t = src; src = dst; dst = t;
+    }
+    plain_realpost<<<blocks_for(uint64_t(lp.M) + 1, kBlock), kBlock, 0, s>>>(src, a.fft, a.power, lp.M, lp.n, lp.rl_hi,
+                                                                         lp.rl_lo);
+    if (ev) cudaEventRecord(ev[2], s);
+    if (ev) cudaEventRecord(ev[3], s);
+    plain_harmonic<<<dim3(blocks_for(p.fundamental, kBlock), 5), kBlock, 0, s>>>(a.power, p, a.summed, a.count,
+                                                                                 a.cands, a.status);
+    if (ev) cudaEventRecord(ev[4], s);
+}
+
+// Gathers the candidates of `count` result slots back to back:
+// offsets[t] = sum of min(counts[u], capacity) for u < t, offsets[count] = total.
+__global__ void bank_compact_kernel(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity,
+                                    uint32_t count, brp_candidate* out, uint64_t out_cap, uint64_t* offsets) {
+    __shared__ uint64_t s_off;
+    // Serial prefix by one thread (count is at most a few thousand).
+    if (threadIdx.x == 0) {
+        uint64_t acc = 0;
+        for (uint32_t t = 0; t < count; ++t) {
+            offsets[t] = acc;
+            acc += counts[t] < capacity ? counts[t] : capacity;
+        }
+        offsets[count] = acc;
+    }
+    __syncthreads();
+    for (uint32_t t = blockIdx.x; t < count; t += gridDim.x) {
+        if (threadIdx.x == 0) s_off = offsets[t];
+        __syncthreads();
+        const uint32_t c = counts[t] < capacity ? counts[t] : capacity;
+        for (uint32_t k = threadIdx.x; k < c; k += blockDim.x)
+            if (s_off + k < out_cap) out[s_off + k] = cands[size_t(t) * capacity + k];
+        __syncthreads();
+    }
+}
+
+void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
+                         brp_candidate* out, uint64_t out_cap, uint64_t* offsets, cudaStream_t s) {
+    bank_compact_kernel<<<1, 256, 0, s>>>(counts, cands, capacity, count, out, out_cap, offsets);
+}
+
+}  // namespace brp

@@ -1,0 +1,111 @@
+// Length plans: the FFT decomposition chosen for one series length n and its
+// twiddle tables.  Every table entry is computed in FP64 (cos/sin of an exact
+// rational angle) and rounded once to FP32; no recurrences.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include "brp_internal.h"
+
+namespace brp {
+
+static bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+static uint32_t ilog2(uint32_t x) { uint32_t r = 0; while (x > 1) { x >>= 1; ++r; } return r; }
+
+// Radix plan of a shared-memory FFT of length L = 2^a or 3*2^a: ceil(a/4)
+// power-of-two passes with the bits spread evenly (radix 16, 8, 4, 2), and a
+// radix-3 pass last when L has the factor 3.
+RadixPlanHost radix_plan(uint32_t L) {
+    RadixPlanHost p;
+    uint32_t three = (L % 3 == 0) ? 1 : 0;
+    uint32_t a = ilog2(L / (three ? 3 : 1));
+    uint32_t passes = (a + 3) / 4;
+    for (uint32_t i = 0; i < passes; ++i) {
+        uint32_t bits = a / passes + (i < a % passes ? 1 : 0);
+        p.radix[p.count++] = 1 << bits;
+    }
+    if (three) p.radix[p.count++] = 3;
+    return p;
+}
+
+static void fill_twiddles(float2* out, uint32_t count, uint64_t period, uint64_t first, uint64_t step) {
+    for (uint32_t i = 0; i < count; ++i) {
+        // angle = -2 pi e / period with e reduced exactly in integers
+        uint64_t e = (first + uint64_t(i) * step) % period;
+        double ang = -2.0 * M_PI * (double(e) / double(period));
+        out[i] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
+    }
+}
+
+size_t plan_smem_limit() { return 110 * 1024; }
+
+std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
+    const bool radix3 = !is_pow2(n);
+    if (n < 64 || n > 3u * (1u << 22) || (radix3 && !(n % 3 == 0 && is_pow2(n / 3))))
+        return "series length must be 2^k or 3*2^k in 64..3*2^22";
+    lp = LengthPlan();
+    lp.n = n;
+    lp.M = n / 2;
+    lp.radix = radix3 ? 3 : 1;
+    lp.B = lp.M / lp.radix;
+    lp.planB = radix_plan(lp.B);
+    // Fused two-pass decomposition for M >= 4096: L2 = 2^min(10, a/2) (a = log2 of
+    // the power-of-two part of M), L1 = M / L2 <= 4096.
+    if (lp.M >= 4096) {
+        uint32_t a = ilog2(lp.B);
+        uint32_t l2 = 1u << std::min<uint32_t>(10, a / 2);
+        while (lp.M / l2 > 4096) l2 <<= 1;
+        lp.L2 = l2;
+        lp.L1 = lp.M / l2;
+        // Elements held per thread (512 threads): 16, or 24 for the longest columns.
+        lp.maxe = lp.L1 * 4 <= 16 * 512 ? 16 : 24;
+        uint32_t cap = lp.maxe * 512;
+        uint32_t C = 16;
+        while (C > 1 && (C * lp.L1 > cap || C > lp.L2 || C * (lp.L1 + lp.L1 / 16 + 16) * 8 > plan_smem_limit())) C >>= 1;
+        uint32_t R = 8;
+        while (R > 1 && (2 * R * lp.L2 > cap || R > lp.L1 / 2 || 2 * R * (lp.L2 + lp.L2 / 16 + 16) * 8 > plan_smem_limit()))
+            R >>= 1;
+        lp.C = C;
+        lp.R = R;
+        lp.plan1 = radix_plan(lp.L1);
+        lp.plan2 = radix_plan(lp.L2);
+        lp.fused = C >= 2 && (lp.L1 / (2 * R)) * 2 * R == lp.L1;
+        if (lp.fused && set_fused_attributes(std::max(lp.smem1(), lp.smem2())) != cudaSuccess)
+            return "cannot enable the shared memory of the fused kernels";
+    }
+    // Tables: tw1[L1] tw2[L2] fs_hi[ceil(M/2048)] fs_lo[2048] rl_hi[ceil(n/2048)] rl_lo[2048] twb[B]
+    const uint32_t split = 1u << kSplitLog2;
+    const uint32_t fs_hi_n = (lp.M + split - 1) / split, rl_hi_n = (n + split - 1) / split;
+    std::vector<size_t> off(8, 0);
+    size_t total = 0;
+    const uint32_t counts[7] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, lp.B};
+    for (int i = 0; i < 7; ++i) { off[i] = total; total += counts[i]; }
+    std::vector<float2> host(total);
+    if (lp.L1) fill_twiddles(host.data() + off[0], lp.L1, lp.L1, 0, 1);
+    if (lp.L2) fill_twiddles(host.data() + off[1], lp.L2, lp.L2, 0, 1);
+    fill_twiddles(host.data() + off[2], fs_hi_n, lp.M, 0, split);
+    fill_twiddles(host.data() + off[3], split, lp.M, 0, 1);
+    fill_twiddles(host.data() + off[4], rl_hi_n, n, 0, split);
+    fill_twiddles(host.data() + off[5], split, n, 0, 1);
+    fill_twiddles(host.data() + off[6], lp.B, lp.B, 0, 1);
+    lp.tables_bytes = total * sizeof(float2);
+    if (cudaMalloc(&lp.d_tables, lp.tables_bytes) != cudaSuccess) return "cudaMalloc of twiddle tables failed";
+    if (cudaMemcpyAsync(lp.d_tables, host.data(), lp.tables_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+        return "upload of twiddle tables failed";
+    lp.tw1 = lp.d_tables + off[0];
+    lp.tw2 = lp.d_tables + off[1];
+    lp.fs_hi = lp.d_tables + off[2];
+    lp.fs_lo = lp.d_tables + off[3];
+    lp.rl_hi = lp.d_tables + off[4];
+    lp.rl_lo = lp.d_tables + off[5];
+    lp.twb = lp.d_tables + off[6];
+    return "";
+}
+
+void free_length_plan(LengthPlan& lp) {
+    if (lp.d_tables) cudaFree(lp.d_tables);
+    lp.d_tables = nullptr;
+}
+
+}  // namespace brp

@@ -1,0 +1,173 @@
+/*
+ * brp_cuda.h -- C ABI of the B200 (sm_100a) backend for the BRP4 per-template
+ * search path: orbital resampling, mean padding, packed real FFT, normalized
+ * power spectrum, 1/2/4/8/16-harmonic summing, candidate compaction.
+ *
+ * The entry points replace the Vulkan backend src/vulkan.cpp of
+ * void-512/boinc-einstein-bpr4-v3d behind its unchanged C++ interface
+ * include/brp/vulkan.hpp (class brp::GPU).  The package's
+ * csrc/brp_gpu_adapter.cpp implements brp::GPU on top of these functions, so
+ * the reference's brp_bench (src/main.cpp) and brp_workunit
+ * (src/workunit_main.cpp) link against this library unmodified.
+ *
+ * Conventions: every function returns an int status (BRP_OK, or a BRP_E* code),
+ * never throws, never exits; brp_cuda_last_error() gives the message of the
+ * last failure of a context (or of the calling thread for a NULL context).
+ * Plain pointers and sizes only; all host buffers are caller owned.
+ */
+#ifndef BRP_CUDA_H
+#define BRP_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BRP_CUDA_ABI_VERSION 1
+
+/* Status codes.  BRP_E_RUNTIME maps to the reference's std::runtime_error
+ * (exit code 1 of src/main.cpp:118); BRP_E_RESULT is a device error word set by
+ * a kernel (resample index outside the observation, candidate overflow;
+ * src/vulkan.cpp:333); BRP_E_TIMEOUT a host wait that reached its deadline. */
+enum { BRP_OK = 0, BRP_E_RUNTIME = 1, BRP_E_RESULT = 2, BRP_E_TIMEOUT = 3, BRP_E_ARGUMENT = 4 };
+
+/* Per-template device error word bits (shaders/resample.comp:18,
+ * shaders/harmonic.comp:34). */
+enum { BRP_STATUS_OVERFLOW = 1u, BRP_STATUS_RESAMPLE_OOB = 2u };
+
+/* Byte-identical to brp::Params (include/brp/science.hpp:8-17, 108 bytes). */
+typedef struct brp_params {
+    uint32_t n, unpadded, steps, logn;
+    float tau, omega, psi, dt, step_inv, s0;
+    uint32_t fundamental, harmonic, window, stage;
+    float threshold[5];
+    uint32_t capacity;
+    uint32_t fft_n, fft_base, fft_radix, flags, twiddle3, twiddle_real;
+    uint32_t result_slot;
+} brp_params;
+
+/* Params.flags bits the backend honours.  Bit 2 selects the FMA resampling
+ * arithmetic of src/science.cpp:29-38 (bit 4, the V3D FMA emulation of
+ * shaders/common.glsl:43-58, is the same correctly rounded FMA here).
+ * BRP_FLAG_INDEX_FP64 is an extension: the time index t + tau*sin(Omega*t+psi)
+ * in FP64 with a libm-accurate sine instead of the FP32 LUT (it does not match
+ * the reference's indices bit for bit and reports its own mismatch count). */
+enum { BRP_FLAG_PACKED = 1u, BRP_FLAG_FMA = 2u, BRP_FLAG_FMA_EMULATED = 4u, BRP_FLAG_INDEX_FP64 = 256u };
+
+/* brp::Candidate (include/brp/science.hpp:18). */
+typedef struct brp_candidate { uint32_t bin, level; float power; uint32_t reserved; } brp_candidate;
+
+/* The constructor options of brp::GPU (include/brp/vulkan.hpp:13;
+ * src/vulkan.cpp:278-284).  The reference's algorithm switches (stockham,
+ * radix4, radix8, ...) are validated with the reference's rules and recorded;
+ * the results do not depend on them here. */
+enum {
+    BRP_OPT_SOFTWARE = 1u, BRP_OPT_STOCKHAM = 2u, BRP_OPT_RADIX4 = 4u, BRP_OPT_PACKED = 8u,
+    BRP_OPT_SCATTER = 16u, BRP_OPT_RADIX8 = 32u, BRP_OPT_FUSED_POWER = 64u, BRP_OPT_RADIX8_STORE = 128u,
+    /* Extension: run the step-by-step per-template pipeline (one kernel per
+     * stage, global-memory FFT passes) instead of the fused pipeline. */
+    BRP_OPT_PLAIN = 1u << 16
+};
+typedef struct brp_options {
+    uint32_t workgroup; /* 1..256, as src/vulkan.cpp:121 */
+    uint32_t tile;      /* 0 or a power of two in 64..4096 (src/vulkan.cpp:121) */
+    uint32_t batch;     /* 1..64 templates per run (src/vulkan.cpp:121) */
+    uint32_t flags;     /* BRP_OPT_* */
+    int32_t device;     /* CUDA device ordinal; -1 = the calling thread's current device */
+    uint32_t reserved[3];
+} brp_options;
+
+/* brp::Timings (include/brp/vulkan.hpp:6).  stage_ms: resample+pad, FFT,
+ * power, harmonic+candidates, summed over the templates of the run. */
+typedef struct brp_timings { double wall_ms, cpu_ms, submit_ms; double stage_ms[4]; } brp_timings;
+
+typedef struct brp_ctx brp_ctx;
+
+/* Replaces brp::GPU::GPU / GPU::Impl::init (src/vulkan.cpp:109-214, :278-284).
+ * Copies input[unpadded] to the device. */
+int brp_cuda_create(const brp_params* params, const float* input, uint32_t unpadded, const brp_options* options,
+                    brp_ctx** out);
+/* Replaces GPU::~GPU (src/vulkan.cpp:38-56). */
+void brp_cuda_destroy(brp_ctx* ctx);
+/* Replaces GPU::set_templates / set_template (src/vulkan.cpp:286-295, :270-276):
+ * 1..batch templates with the constructor's n, unpadded, fundamental, harmonic,
+ * capacity and arithmetic flags. */
+int brp_cuda_set_templates(brp_ctx* ctx, const brp_params* templates, uint32_t count);
+/* Replaces GPU::run (src/vulkan.cpp:296-318): runs every template set, blocks
+ * until done.  template_stage_ms (optional) receives count*4 doubles. */
+int brp_cuda_run(brp_ctx* ctx, brp_timings* timings, double* template_stage_ms);
+/* Replaces GPU::snapshot (src/vulkan.cpp:319-328) for the last template of the
+ * last run.  Any pointer may be NULL.  resampled: n floats (steps values then
+ * the mean); fft: 2*(n/2+1) floats; power: n/2 floats; summed: 5*fundamental. */
+int brp_cuda_snapshot(brp_ctx* ctx, float* resampled, float* fft, float* power, float* summed);
+/* Replaces GPU::candidates (src/vulkan.cpp:329-337): the candidates of one
+ * result slot sorted by (level, bin); slot UINT32_MAX = the last template.
+ * *count receives the full count even when it exceeds cap.  Returns
+ * BRP_E_RESULT when the slot's error word is set (overflow or resample OOB). */
+int brp_cuda_candidates(brp_ctx* ctx, uint32_t slot, brp_candidate* out, uint32_t cap, uint32_t* count);
+/* Replaces GPU::device_info / allocated_bytes / profile_counters
+ * (src/vulkan.cpp:338-346).  Counters are a JSON string of per-stage event times. */
+int brp_cuda_device_info(brp_ctx* ctx, char* buffer, size_t length);
+uint64_t brp_cuda_allocated_bytes(const brp_ctx* ctx);
+int brp_cuda_profile_counters(brp_ctx* ctx, char* buffer, size_t length);
+const char* brp_cuda_last_error(const brp_ctx* ctx);
+
+/* ---- Bank extension: a whole orbital bank over series of different lengths,
+ * run as one captured CUDA graph (the batched form of src/workunit_main.cpp:77-93).
+ * No reference counterpart beyond that loop; candidates per template are those
+ * GPU::candidates would return. ---- */
+typedef struct brp_bank brp_bank;
+/* series_count series; series s has unpadded[s] samples padded to n[s]
+ * (a power of two or 3*2^k, 64..3*2^22).  max_templates bounds one run;
+ * capacity is the candidate capacity of each template's result slot. */
+int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, const uint32_t* unpadded, uint32_t max_templates,
+                         uint32_t capacity, int32_t device, brp_bank** out);
+void brp_cuda_bank_destroy(brp_bank* bank);
+/* Copies one series (unpadded[s] floats, host memory) to the device. */
+int brp_cuda_bank_set_series(brp_bank* bank, uint32_t series, const float* input);
+/* Runs count templates; template t searches series series_of[t] with
+ * templates[t] (whose n/unpadded must equal that series').  Writes the
+ * candidates of all templates back to back into out (sorted by (level, bin)
+ * within a template), counts[t] per template and status[t] (BRP_STATUS_* bits).
+ * out_cap bounds the total; BRP_E_RESULT if a template's status is non-zero or
+ * out_cap is too small.  Blocks until done. */
+int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count,
+                      brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status);
+/* Device-only replay of the last brp_cuda_bank_run's graph (no host copies,
+ * no wait): the throughput kernel time is measured around this by the caller
+ * with events on brp_cuda_bank_stream(). */
+int brp_cuda_bank_launch(brp_bank* bank);
+void* brp_cuda_bank_stream(brp_bank* bank);
+/* Kernels launched by one replay (for launch accounting). */
+uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* bank);
+const char* brp_cuda_bank_last_error(const brp_bank* bank);
+
+/* ---- Host helpers (the reference's host code around the path) ---- */
+/* src/science.cpp:46-65 (brp::parameters). */
+int brp_host_parameters(uint32_t n, uint32_t unpadded, float tau, float period, float psi, float dt,
+                        brp_params* out);
+/* src/science.cpp:41-45 (brp::resampling_steps). */
+int brp_host_resampling_steps(brp_params* p);
+/* src/workload.cpp:108-125 (brp::search_parameters); n, samples and sample_us
+ * describe the observation. */
+int brp_host_search_parameters(uint32_t n, uint32_t samples, double sample_us, double period, double tau,
+                               double psi, double f0, double false_alarm, uint32_t window, brp_params* out);
+
+/* src/workload.cpp:126-159 (brp::Toplist). */
+typedef struct brp_bank_candidate {
+    double power, period, tau, psi, significance;
+    uint32_t harmonics, bin;
+} brp_bank_candidate;
+typedef struct brp_toplist brp_toplist;
+brp_toplist* brp_toplist_create(void);
+void brp_toplist_destroy(brp_toplist* t);
+void brp_toplist_thresholds(const brp_toplist* t, brp_params* p);
+int brp_toplist_retain(brp_toplist* t, const brp_candidate* candidates, uint32_t count, double period, double tau,
+                       double psi, const brp_params* p);
+/* Writes up to 100 final candidates; returns how many. */
+uint32_t brp_toplist_final(const brp_toplist* t, brp_bank_candidate* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

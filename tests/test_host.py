@@ -1,0 +1,110 @@
+"""Host-side logic of the product (template constants, search parameters,
+toplist) against the CPU oracle and, where built, the reference's own
+compiled code.  No GPU needed: these are host functions of libbrp_cuda.so."""
+import numpy as np
+import pytest
+
+import brp_b200 as B
+from brp_b200 import synth
+
+CASES = [
+    (65536, 65536 - 17, 0.002, 120.0, 0.3, 256e-6),
+    (65536, 65536 - 17, 0.3, 3600.0, 1.1, 128e-6),
+    (1 << 22, (1 << 22) - 17, 1.7, 11 * 3600.0, 0.4, 128e-6),
+    (3 << 21, 3 << 21, 3.0, 3600.0, -5.0, 128e-6),
+    (64, 47, 0.0, 10.0, 0.0, 1e-3),
+    (96, 64, 1e-3, 1.0, 6.2, 1e-3),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_parameters_match_oracle(oracle, case):
+    p = B.parameters(*case)
+    q = oracle.parameters(*case)
+    assert bytes(p) == bytes(q)
+    assert bytes(B.production(p)) == bytes(oracle.production(q))
+
+
+@pytest.mark.parametrize("bad", [(63, 60, 0.1, 1.0, 0.0, 1e-3), (100, 90, 0.1, 1.0, 0.0, 1e-3),
+                                 (64, 65, 0.1, 1.0, 0.0, 1e-3), (64, 60, -1.0, 1.0, 0.0, 1e-3),
+                                 (64, 60, 0.1, 0.0, 0.0, 1e-3), (64, 60, 0.1, 1.0, float("nan"), 1e-3)])
+def test_parameters_reject_like_reference(oracle, bad):
+    with pytest.raises(B.BrpError):
+        B.parameters(*bad)
+    with pytest.raises(oracle.OracleError):
+        oracle.parameters(*bad)
+
+
+@pytest.mark.parametrize("orbit", [(3600.0, 0.3, 1.1), (86000.0, 2.9, 4.0), (20000.0, 0.0, 0.0)])
+@pytest.mark.parametrize("obs", [(1 << 22, 1 << 22), (3 << 20, 3 << 20), (1 << 20, 900000)])
+def test_search_parameters_match_oracle(oracle, orbit, obs):
+    n, samples = obs
+    for f0, fa, w in [(400.0, 0.08, 1000), (800.0, 0.01, 500), (50.0, 1e-6, 7)]:
+        p = B.search_parameters(n, samples, 128.0, *orbit, f0, fa, w)
+        q = oracle.search_parameters(n, samples, 128.0, *orbit, f0, fa, w)
+        assert bytes(p) == bytes(q)
+
+
+def test_search_parameters_match_reference(oracle):
+    if not oracle.ref_available():
+        pytest.skip("reference build absent (oracle/_ref)")
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        P, tau, psi = synth.random_orbits(rng, 1)[0]
+        p = B.search_parameters(1 << 22, 1 << 22, 128.0, P, tau, psi, 400.0, 0.08, 1000)
+        r = oracle.ref_search_parameters(1 << 22, 1 << 22, 128.0, P, tau, psi, 400.0, 0.08, 1000)
+        assert bytes(p) == bytes(r)
+
+
+def test_sigma_false_alarm_thresholds():
+    n = 1 << 20
+    p5 = B.search_parameters(n, n, 128.0, 3600.0, 0.5, 0.1, 400.0, synth.sigma_false_alarm(n, 5.0), 1000)
+    p7 = B.search_parameters(n, n, 128.0, 3600.0, 0.5, 0.1, 400.0, synth.sigma_false_alarm(n, 7.0), 1000)
+    # level 0 threshold = -ln(p): 5 sigma tail 2.87e-7 -> 15.06, 7 sigma 1.28e-12 -> 27.4
+    assert abs(p5.threshold[0] - 15.06) < 0.05
+    assert abs(p7.threshold[0] - 27.38) < 0.05
+    assert all(a < b for a, b in zip(p5.threshold, p7.threshold))
+
+
+def _random_candidates(rng, p, count):
+    bins = rng.integers(p.window, p.fundamental, count)
+    levels = rng.integers(0, 5, count)
+    thr = np.asarray(list(p.threshold))
+    power = (thr[levels] * rng.uniform(0.9, 3.0, count)).astype(np.float32)
+    c = np.zeros(count, B.CANDIDATE)
+    c["bin"], c["level"], c["power"] = bins, levels, power
+    order = np.lexsort((c["bin"], c["level"]))
+    return c[order]
+
+
+def test_toplist_matches_oracle_and_reference(oracle):
+    rng = np.random.default_rng(11)
+    p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
+    tops = [B.Toplist(), oracle.Toplist()]
+    if oracle.ref_available():
+        tops.append(oracle.RefToplist())
+    for t in range(300):
+        c = _random_candidates(rng, p, int(rng.integers(0, 40)))
+        # duplicate bins and exactly equal powers exercise the qsort tie order
+        if t % 7 == 0 and len(c) > 2:
+            c["power"][1] = c["power"][0]
+            c["bin"][2] = c["bin"][0]
+        orb = (3600.0 + t, 0.01 * t, 0.1 * t)
+        for tl in tops:
+            q = tl.thresholds(p)
+            tl.retain(c, *orb, q)
+        qs = [bytes(tl.thresholds(p)) for tl in tops]
+        assert all(q == qs[0] for q in qs)
+    finals = [tl.final() for tl in tops]
+    for f in finals[1:]:
+        assert f.tobytes() == finals[0].tobytes()
+    assert len(finals[0]) > 0
+
+
+def test_toplist_rejects_invalid_candidate():
+    p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
+    t = B.Toplist()
+    c = np.zeros(1, B.CANDIDATE)
+    c["bin"], c["level"], c["power"] = p.fundamental, 0, 100.0
+    with pytest.raises(B.BrpError):
+        t.retain(c, 1.0, 0.0, 0.0, p)
