@@ -1,0 +1,377 @@
+"""Throughput of the BRP4 per-template search on B200.
+
+Workload: the batched bank search at N = 2^22 (one 2^22-sample float32 series
+at 128 us with 3 injected binary pulsars, 512 circular-orbit templates with
+production search parameters, bank-wide toplist of 100), seeded synthetic
+data.  A step is one pass of the search path over the whole bank.
+
+Reported (one JSON line, rank 0):
+  value      templates/s over all ranks, device-resident inputs, one captured
+             CUDA graph per step, L2 flushed between steps (CUDA events on the
+             bank's stream, max over ranks)
+  e2e        the same metric through the public API (Bank.run) with the
+             series copied from pinned host memory every step, candidates copied
+             back and folded into the bank-wide toplist on the host
+  roofline   the dominant kernel's algorithmic bytes / its device time
+  plain      templates/s of the step-by-step per-template pipeline, same GPU
+  cpu_baseline  the reference CPU path on a bounded sample (rank 0, N = 1)
+
+`--impl reference` times the reference's own CPU implementation of the path
+(oracle/_ref: src/science.cpp resampling, the harmonic summing restatement,
+select) with scipy's float32 real FFT standing in for FFTW, over all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "boinc-einstein-bpr4-v3d_b200")
+for _p in (ROOT, PKG_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+N = 1 << 22
+TEMPLATES = 512
+CAPACITY = 8192
+METRIC = "orbital templates/s at N=2^22 on 1 B200 (batched bank search)"
+UNIT = "templates/s"
+L2_FLUSH_BYTES = 512 << 20
+# Algorithmic HBM bytes per template (per kernel) at length n: pass 1 gathers the
+# series (4n) and writes the four-step intermediate (4n); pass 2 reads it (4n) and
+# writes the power spectrum (2n); harmonic summing reads the power spectrum (2n).
+ALGO_BYTES = {"pass1": 8, "pass2": 6, "harmonic": 2}
+
+
+def parse():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    a.add_argument("--templates", type=int, default=TEMPLATES)
+    a.add_argument("--no-cpu-baseline", action="store_true")
+    a.add_argument("--no-plain", action="store_true")
+    return a.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def measured_traffic():
+    """Per-template DRAM bytes of each kernel from the committed ncu summary
+    (profiles/traffic.txt: lines `kernel bytes_per_template`), if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    out = {}
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and not line.startswith("#"):
+                    out[parts[0]] = float(parts[1])
+    except OSError:
+        pass
+    return out
+
+
+# ------------------------------------------------------------------ workload
+def workload(total_templates):
+    from brp_b200 import synth
+    return synth.bank_workload("bank-2^22", [N], [total_templates], [3], seed=3)
+
+
+# --------------------------------------------------------------- CPU baseline
+_W = {}
+
+
+def _cpu_init(series):
+    from oracle import oracle as O
+    import scipy.fft  # noqa: F401
+    _W["x"] = series
+    _W["O"] = O
+    O.ref() if O.ref_available() else O.lib()
+
+
+def _cpu_template(pbytes):
+    """One template through the reference CPU path; returns the candidate count."""
+    import scipy.fft
+    O = _W["O"]
+    p = O.Params.from_buffer_copy(pbytes)
+    x = _W["x"]
+    if O.ref_available():
+        r = O.ref_resample(x, p)
+    else:
+        r = O.resample(x, p)
+    X = scipy.fft.rfft(r, workers=1)  # float32 FFT, the FFTW stand-in
+    n = p.n
+    P = ((X.real[: n // 2].astype(np.float64) ** 2 + X.imag[: n // 2].astype(np.float64) ** 2)
+         * float(np.float32(1.0) / np.float32(n))).astype(np.float32)
+    P[0] = 0
+    S = O.ref_harmonic(P, p) if O.ref_available() else O.harmonic(P, p)
+    return len(O.select(S, p))
+
+
+def cpu_pool(series, cores):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    return ctx.Pool(cores, initializer=_cpu_init, initargs=(series,))
+
+
+def time_cpu(pool, templates, sample):
+    blobs = [bytes(templates[k % len(templates)]) for k in range(sample)]
+    t0 = time.perf_counter()
+    pool.map(_cpu_template, blobs, chunksize=1)
+    return time.perf_counter() - t0
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_kind():
+    from oracle import oracle as O
+    return "reference" if O.ref_available() else "port"
+
+
+# ------------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device_index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows]
+        mx = max(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip().lower() == "active"})
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    wl = workload(args.templates)
+    cores = host_cores()
+    pool = cpu_pool(wl.series[0], cores)
+    sample = max(cores, 16)
+    for _ in range(max(args.warmup, 1)):
+        time_cpu(pool, wl.templates, min(sample, cores))
+    times = [time_cpu(pool, wl.templates, sample) for _ in range(args.steps)]
+    pool.close()
+    total = sum(times)
+    value = sample * args.steps / total
+    kind = reference_kind()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "bank search, N=2^22, %d templates (sample of %d per step)" % (args.templates, sample),
+                       "n": N, "templates": args.templates},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": "%d templates of the N=2^22 bank per step over %d processes" % (sample, cores)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- CUDA arm
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    total_templates = args.templates * world
+    wl = workload(total_templates)
+    from brp_b200 import shard
+    begin, end = shard.shard_range(total_templates, rank, world)
+    my_templates = wl.templates[begin:end]
+    count = len(my_templates)
+
+    # The CPU pool is started before the first GPU call (spawned workers).
+    pool = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pool = cpu_pool(wl.series[0], host_cores())
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import brp_b200 as B
+
+    bank = B.Bank([N], [N], count, CAPACITY, device=local)
+    series = torch.from_numpy(wl.series[0]).pin_memory()
+    x_host = series.numpy()
+    stream = torch.cuda.ExternalStream(bank.stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def e2e_step():
+        bank.set_series(0, x_host)
+        cands, counts, status = bank.run(my_templates)
+        return cands
+
+    # warm-up through the public API (captures the graph)
+    for _ in range(max(args.warmup, 3)):
+        cands = e2e_step()
+    d2h = 4 * count * 2 + 8 * (count + 1) + 16 * sum(len(c) for c in cands)
+    h2d = 4 * N + 108 * count + 8 * count
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- device throughput (value)
+    clocks = Clocks(local)
+    barrier()
+    step_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bank.launch()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    barrier()
+    clock = clocks.stop()
+    dev_ms = sum(step_ms)
+
+    # --- end to end through the public API (series H2D + candidates D2H + toplist)
+    barrier()
+    t0 = time.perf_counter()
+    top = B.Toplist()
+    for _ in range(args.steps):
+        cands = e2e_step()
+        if world == 1:
+            shard.fold_toplist(top, my_templates, wl.orbits[begin:end], cands)
+    torch.cuda.synchronize()
+    e2e_ms = 1000 * (time.perf_counter() - t0)
+    barrier()
+
+    # per-kernel device time of one eager replay (roofline)
+    kernel_ms, launches = bank.profile()
+
+    if dist:
+        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, e2e_ms = t.tolist()
+
+    # plain per-template pipeline on the same GPU (comparator)
+    plain = None
+    if rank == 0 and not args.no_plain:
+        plain = time_plain(B, wl, my_templates[:8])
+
+    cpu = None
+    if pool is not None:
+        cores = host_cores()
+        sample = 64
+        time_cpu(pool, wl.templates, min(cores, sample))
+        secs = time_cpu(pool, wl.templates, sample)
+        pool.close()
+        cpu = {"value": sample / secs, "unit": UNIT, "cores": cores, "kind": reference_kind(),
+               "sample": "%d templates of the N=2^22 bank over %d processes (scipy float32 rfft for FFTW)" % (
+                   sample, cores)}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = load_peaks()
+    per_launch = {k: kernel_ms[k] / max(launches[k], 1) for k in ("pass1", "pass2", "harmonic")}
+    top_kernel = max(per_launch, key=lambda k: kernel_ms[k])
+    group = count / max(launches[top_kernel], 1)
+    algo = ALGO_BYTES[top_kernel] * N * group
+    achieved = algo / (per_launch[top_kernel] * 1e-3) / 1e9
+    traffic = measured_traffic().get(top_kernel)
+    value = total_templates * args.steps / (dev_ms / 1000)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "bank search, N=2^22, %d templates per GPU, 3 injected pulsars" % args.templates,
+                   "n": N, "templates_per_gpu": count, "candidate_capacity": CAPACITY,
+                   "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
+                   "parallelism": "template shards, %d rank(s)" % world},
+        "e2e": {"value": total_templates * args.steps / (e2e_ms / 1000), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": bank.kernels_per_run * args.steps,
+        "roofline": {"bound": "hbm", "kernel": top_kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic * group if traffic else None,
+                     "algorithmic_bytes_per_launch": algo, "templates_per_launch": group},
+        "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": launches,
+        "algorithmic_gbs_all_kernels": 16 * N * count / (sum(kernel_ms[k] for k in ALGO_BYTES) * 1e-3) / 1e9,
+        "clocks": clock,
+    }
+    if plain:
+        line["plain"] = plain
+        line["batched_vs_plain"] = value / world / plain["templates_per_s"]
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def time_plain(B, wl, templates):
+    """Device time per template of the step-by-step pipeline (batch 1), and of
+    the fused pipeline run one template at a time through brp::GPU."""
+    out = {}
+    for name, plain in (("templates_per_s", True), ("fused_single_templates_per_s", False)):
+        g = B.GPU(templates[0], wl.series[0], 256, 0, 1, stockham=True, packed=True, plain=plain)
+        ms = []
+        for k, p in enumerate(templates):
+            g.set_template(p)
+            t = g.run()
+            if k >= 2:
+                ms.append(sum(t.stage_ms))
+        g.close()
+        out[name] = 1000.0 / statistics.mean(ms)
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -56,8 +56,8 @@ class Bank:
         st = lib().brp_cuda_bank_run(self._b, arr, ptr(so), count, ptr(out), out.size, ptr(counts), ptr(status))
         if st and st != 2:
             check(st, self._err)
-        kept = np.minimum(counts, self.capacity)
-        offs = np.concatenate([[0], np.cumsum(kept)])
+        offs = np.zeros(count + 1, np.int64)
+        offs[1:] = np.cumsum(np.minimum(counts, self.capacity).astype(np.int64))
         result = [out[offs[t]:offs[t + 1]].copy() for t in range(count)]
         if st:
             e = BrpError(st, self._err())
@@ -68,6 +68,15 @@ class Bank:
     def launch(self):
         """Replays the last run's graph on the device only (no copies, no wait)."""
         check(lib().brp_cuda_bank_launch(self._b), self._err)
+
+    def profile(self):
+        """Per-kernel device time of one eager replay of the last run:
+        ({"pass1", "pass2", "harmonic", "compact"} -> ms, launches per kind)."""
+        ms = np.zeros(4, np.float64)
+        launches = np.zeros(4, np.uint32)
+        check(lib().brp_cuda_bank_profile(self._b, ptr(ms), ptr(launches)), self._err)
+        names = ("pass1", "pass2", "harmonic", "compact")
+        return dict(zip(names, ms.tolist())), dict(zip(names, launches.tolist()))
 
     @property
     def stream(self):

@@ -1,0 +1,46 @@
+"""Bank sharding across ranks (one process per GPU).
+
+Templates are independent and the observation is read-only, so a bank splits
+into contiguous template ranges, one per rank, with no data-path collective.
+The bank-wide toplist is a sequential fold over templates in bank order
+(src/workload.cpp:126-141); it is built after the search from every rank's
+compact candidate lists, gathered to rank 0.  Because each template's
+candidates are compacted against its own (start-of-bank) thresholds and the
+toplist re-filters them against its current rows, the final toplist equals the
+single-GPU one (batch invariance, src/workunit_main.cpp:85-93).
+"""
+import numpy as np
+
+
+def shard_range(count, rank, world):
+    """Contiguous [begin, end) of `count` templates for `rank` of `world`."""
+    base, extra = divmod(count, world)
+    begin = rank * base + min(rank, extra)
+    return begin, begin + base + (1 if rank < extra else 0)
+
+
+def gather_candidates(per_template, begin, group=None):
+    """Gathers {template index: candidates} from every rank to rank 0 over
+    torch.distributed (gloo or nccl object collectives).  Returns the merged
+    list in bank order on rank 0, None elsewhere."""
+    import torch.distributed as dist
+    payload = {begin + k: np.asarray(c).tobytes() for k, c in enumerate(per_template)}
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    out = [None] * world if rank == 0 else None
+    dist.gather_object(payload, out, dst=0, group=group)
+    if rank != 0:
+        return None
+    from ._lib import CANDIDATE
+    merged = {}
+    for d in out:
+        merged.update(d)
+    return [np.frombuffer(merged[t], dtype=CANDIDATE) for t in sorted(merged)]
+
+
+def fold_toplist(toplist, templates, orbits, candidates):
+    """Retains every template's candidates in bank order (src/workunit_main.cpp:124)."""
+    for p, orb, c in zip(templates, orbits, candidates):
+        q = toplist.thresholds(p)
+        toplist.retain(c, orb[0], orb[1], orb[2], q)
+    return toplist

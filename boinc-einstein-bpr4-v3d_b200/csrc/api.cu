@@ -419,6 +419,8 @@ struct brp_bank {
     cudaGraphExec_t exec = nullptr;
     std::vector<uint64_t> graph_key;
     uint32_t kernels_per_run = 0;
+    std::vector<uint32_t> last_sorted_n, last_spans;
+    uint32_t last_count = 0;
     cudaEvent_t done = nullptr;
     std::string error;
 
@@ -533,9 +535,20 @@ extern "C" int brp_cuda_bank_set_series(brp_bank* b, uint32_t s, const float* in
                    "series upload");
 }
 
-// Records the whole bank search on b->stream (captured into the graph).
+// Records the whole bank search on b->stream (captured into the graph).  With
+// `prof` (eager replay only) each kernel is bracketed by events: prof->push_back
+// gets (kind, start, end) with kind 0 = pass 1, 1 = pass 2, 2 = harmonic, 3 = compaction.
+struct KernelEvents { std::vector<int> kind; std::vector<cudaEvent_t> ev; };
 static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, const std::vector<uint32_t>& spans,
-                        uint32_t count) {
+                        uint32_t count, KernelEvents* prof = nullptr) {
+    auto mark = [&](int kind, bool start) {
+        if (!prof) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, b->stream);
+        prof->ev.push_back(e);
+        if (start) prof->kind.push_back(kind);
+    };
     cudaStream_t s = b->stream;
     cudaMemsetAsync(b->d_counts, 0, count * sizeof(uint32_t), s);
     cudaMemsetAsync(b->d_status, 0, count * sizeof(uint32_t), s);
@@ -564,13 +577,21 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         a.snap = -1;
         uint32_t span = 0;
         for (uint32_t u = t; u < end; ++u) span = std::max(span, spans[u]);
+        mark(0, true);
         launch_fused_pass1(a, lp, g, s);
+        mark(0, false);
+        mark(1, true);
         launch_fused_pass2(a, lp, g, s);
+        mark(1, false);
+        mark(2, true);
         launch_fused_harmonic(a, lp, g, span, s);
+        mark(2, false);
         kernels += 3;
         t = end;
     }
+    mark(3, true);
     launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_compact, b->compact_cap, b->d_offsets, s);
+    mark(3, false);
     b->kernels_per_run = kernels + 1;
 }
 
@@ -611,6 +632,9 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
         (st = b->cuda(cudaMemcpyAsync(b->d_inputs, b->h_inputs, count * sizeof(void*), cudaMemcpyHostToDevice, s),
                       "inputs upload")))
         return st;
+    b->last_sorted_n = sorted_n;
+    b->last_spans = spans;
+    b->last_count = count;
     if (key != b->graph_key || !b->exec) {
         if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
         if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
@@ -664,6 +688,28 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
 extern "C" int brp_cuda_bank_launch(brp_bank* b) {
     if (!b || !b->exec) return set_thread_error(BRP_E_ARGUMENT, "no captured bank graph");
     return b->cuda(cudaGraphLaunch(b->exec, b->stream), "graph launch");
+}
+
+extern "C" int brp_cuda_bank_profile(brp_bank* b, double* kernel_ms, uint32_t* launches) {
+    if (!b || !kernel_ms || !b->last_count) return set_thread_error(BRP_E_ARGUMENT, "no bank run to profile");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    KernelEvents prof;
+    record_bank(b, b->last_sorted_n, b->last_spans, b->last_count, &prof);
+    cudaEventRecord(b->done, b->stream);
+    bool timed_out = false;
+    cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
+    if (timed_out) return b->fail(BRP_E_TIMEOUT, "bank profile exceeded its deadline");
+    if ((st = b->cuda(e, "bank profile"))) return st;
+    for (int k = 0; k < 4; ++k) { kernel_ms[k] = 0; if (launches) launches[k] = 0; }
+    for (size_t i = 0; i < prof.kind.size(); ++i) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, prof.ev[2 * i], prof.ev[2 * i + 1]);
+        kernel_ms[prof.kind[i]] += ms;
+        if (launches) launches[prof.kind[i]] += 1;
+    }
+    for (auto ev : prof.ev) cudaEventDestroy(ev);
+    return BRP_OK;
 }
 
 extern "C" void* brp_cuda_bank_stream(brp_bank* b) { return b ? static_cast<void*>(b->stream) : nullptr; }

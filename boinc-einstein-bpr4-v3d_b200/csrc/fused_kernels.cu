@@ -360,10 +360,16 @@ static void launch_p2(const FusedArgs& a, const LengthPlan& lp, uint32_t count, 
     pass2_kernel<MAXE, kThreads><<<dim3(lp.blocks2(), count), kThreads, lp.smem2(), s>>>(a);
 }
 
-// Opts the fused kernels into large dynamic shared memory on the current
-// device (done at plan creation, outside any stream capture).
+// Opts the fused kernels into the device's largest dynamic shared memory per
+// block (done at plan creation, outside any stream capture).  The limit is a
+// per-kernel maximum, so it is set once to the device limit rather than to one
+// plan's need, which a later, smaller plan would otherwise lower.
 cudaError_t set_fused_attributes(size_t max_dynamic_smem) {
-    int v = int(max_dynamic_smem);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (size_t(optin) < max_dynamic_smem + 1024) return cudaErrorInvalidValue;
+    int v = optin - 1024;  // static shared memory of the kernels (reduction scratch) fits in the rest
     cudaError_t e = cudaFuncSetAttribute(pass1_kernel<16, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(pass1_kernel<24, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(pass2_kernel<16, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);

@@ -138,6 +138,12 @@ int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_
  * with events on brp_cuda_bank_stream(). */
 int brp_cuda_bank_launch(brp_bank* bank);
 void* brp_cuda_bank_stream(brp_bank* bank);
+/* Replays the last run's kernels eagerly with an event pair around each launch
+ * and sums the device time per kernel kind: kernel_ms[0] pass 1 (resample +
+ * column FFTs), [1] pass 2 (row FFTs + real spectrum + power), [2] harmonic
+ * summing + compaction, [3] candidate gather.  launches (optional) gets the
+ * launch count per kind. */
+int brp_cuda_bank_profile(brp_bank* bank, double* kernel_ms, uint32_t* launches);
 /* Kernels launched by one replay (for launch accounting). */
 uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* bank);
 const char* brp_cuda_bank_last_error(const brp_bank* bank);
