@@ -57,6 +57,7 @@ def parse():
     a.add_argument("--templates", type=int, default=TEMPLATES)
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-plain", action="store_true")
+    a.add_argument("--no-tune", action="store_true", help="skip the autotuner (default kernels)")
     return a.parse_args()
 
 
@@ -250,7 +251,16 @@ def main():
         cands, counts, status = bank.run(my_templates)
         return cands
 
-    # warm-up through the public API (captures the graph)
+    # autotune the kernel configuration and templates per launch on this bank
+    # (untimed), then warm up through the public API (captures the graph)
+    plan = None
+    if not args.no_tune:
+        from brp_b200 import tune
+        bank.set_series(0, x_host)
+        res = tune.autotune(bank, my_templates, use_cache=False)
+        plan = {str(n): {k: r[k] for k in ("pass1", "pass2", "group", "ms")} for n, r in res.items()}
+        if os.environ.get("BRP_BENCH_VERBOSE"):
+            print(json.dumps({"tuning": {str(n): r.get("tried") for n, r in res.items()}}), file=sys.stderr)
     for _ in range(max(args.warmup, 3)):
         cands = e2e_step()
     d2h = 4 * count * 2 + 8 * (count + 1) + 16 * sum(len(c) for c in cands)
@@ -334,7 +344,8 @@ def main():
         "config": {"workload": "bank search, N=2^22, %d templates per GPU, 3 injected pulsars" % args.templates,
                    "n": N, "templates_per_gpu": count, "candidate_capacity": CAPACITY,
                    "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
-                   "parallelism": "template shards, %d rank(s)" % world},
+                   "parallelism": "template shards, %d rank(s)" % world,
+                   "plan": plan},
         "e2e": {"value": total_templates * args.steps / (e2e_ms / 1000), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": bank.kernels_per_run * args.steps,

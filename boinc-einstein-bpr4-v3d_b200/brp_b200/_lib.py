@@ -73,7 +73,7 @@ EXPORTS = (
     "brp_cuda_create", "brp_cuda_destroy", "brp_cuda_set_templates", "brp_cuda_run", "brp_cuda_snapshot",
     "brp_cuda_candidates", "brp_cuda_device_info", "brp_cuda_allocated_bytes", "brp_cuda_profile_counters",
     "brp_cuda_last_error", "brp_cuda_bank_create", "brp_cuda_bank_destroy", "brp_cuda_bank_set_series",
-    "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
+    "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_configure", "brp_cuda_fast_configs", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
     "brp_cuda_bank_last_error", "brp_host_parameters", "brp_host_resampling_steps", "brp_host_search_parameters",
     "brp_toplist_create", "brp_toplist_destroy", "brp_toplist_thresholds", "brp_toplist_retain",
     "brp_toplist_final",
@@ -113,6 +113,8 @@ def lib():
             L.brp_cuda_bank_set_series.argtypes = [vp, u32, vp]
             L.brp_cuda_bank_run.argtypes = [vp, vp, vp, u32, vp, u64, vp, vp]
             L.brp_cuda_bank_launch.argtypes = [vp]
+            L.brp_cuda_bank_configure.argtypes = [vp, u32, ctypes.c_int32, ctypes.c_int32, u32]
+            L.brp_cuda_fast_configs.argtypes = [vp, vp, vp, u32]
             L.brp_cuda_bank_profile.argtypes = [vp, vp, vp]
             L.brp_cuda_bank_stream.argtypes = [vp]
             L.brp_cuda_bank_stream.restype = vp
@@ -139,6 +141,17 @@ def lib():
 def check(status, message_fn):
     if status:
         raise BrpError(status, message_fn())
+
+
+def fast_configs():
+    """Compiled pass configurations: list of (id, L, kind) with kind 1 = pass 1, 2 = pass 2."""
+    L = lib()
+    n = L.brp_cuda_fast_configs(None, None, None, 0)
+    ids = np.zeros(n, np.int32)
+    lens = np.zeros(n, np.uint32)
+    kinds = np.zeros(n, np.uint32)
+    L.brp_cuda_fast_configs(ptr(ids), ptr(lens), ptr(kinds), n)
+    return [(int(i), int(l), int(k)) for i, l, k in zip(ids, lens, kinds)]
 
 
 def ptr(a):

@@ -19,7 +19,7 @@ UINT32_MAX = 0xFFFFFFFF
 class GPU:
     def __init__(self, params, input, workgroup=192, tile=512, batch=4, software=False, stockham=False,
                  radix4=False, packed=False, scatter=False, radix8=False, fused_power=False, radix8_store=False,
-                 plain=False, device=-1):
+                 plain=False, device=-1, pass1=0, pass2=0):
         L = lib()
         self._ctx = None
         x = np.ascontiguousarray(input, dtype=np.float32)
@@ -30,6 +30,8 @@ class GPU:
             if on:
                 flags |= OPT[name]
         o = Options(workgroup, tile, batch, flags, device)
+        o.reserved[0] = pass1 & 0xFFFFFFFF  # compiled pass configuration ids (-1: generic kernels)
+        o.reserved[1] = pass2 & 0xFFFFFFFF
         ctx = ctypes.c_void_p()
         st = L.brp_cuda_create(ctypes.byref(params), ptr(x), x.size, ctypes.byref(o), ctypes.byref(ctx))
         check(st, lambda: L.brp_cuda_last_error(None).decode())

@@ -172,7 +172,11 @@ extern "C" int brp_cuda_create(const brp_params* params, const float* input, uin
     c->base = p;
     if (options->flags & BRP_OPT_PACKED) c->base.flags |= BRP_FLAG_PACKED;
     c->wg = options->workgroup; c->tile = options->tile; c->batch = options->batch; c->opt = options->flags;
-    std::string e = make_length_plan(p.n, c->lp, c->stream);
+    // reserved[0] / reserved[1]: compiled pass-1 / pass-2 configuration ids
+    // (0 = default choice, UINT32_MAX = generic kernels).
+    const int f1 = options->reserved[0] == UINT32_MAX ? -1 : int(options->reserved[0]);
+    const int f2 = options->reserved[1] == UINT32_MAX ? -1 : int(options->reserved[1]);
+    std::string e = make_length_plan(p.n, c->lp, c->stream, f1, f2);
     if (!e.empty()) { delete c; return set_thread_error(BRP_E_RUNTIME, e); }
     c->fused = c->lp.fused && !(options->flags & BRP_OPT_PLAIN);
     const uint32_t B = c->batch, M = c->lp.M, cap = p.capacity;
@@ -228,10 +232,7 @@ static FusedArgs fused_args(brp_ctx* c, uint32_t count) {
     const LengthPlan& lp = c->lp;
     a.inputs = c->d_inputs;
     a.params = c->d_params;
-    a.n = lp.n; a.M = lp.M; a.L1 = lp.L1; a.L2 = lp.L2; a.C = lp.C; a.R = lp.R;
-    a.plan1[0] = lp.plan1.count; a.plan2[0] = lp.plan2.count;
-    for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
-    a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
+    fill_fused_args(a, lp);
     a.work = c->d_work; a.work_stride = lp.M;
     a.power = c->d_power; a.power_stride = lp.M;
     a.partial = c->d_partial; a.partial_stride = lp.blocks1();
@@ -399,7 +400,14 @@ struct brp_bank {
     std::vector<uint32_t> n, unpadded;
     std::vector<float*> d_series;
     std::map<uint32_t, LengthPlan> plans;  // by n
-    struct ClassBuffers { float2* work = nullptr; float* power = nullptr; double* partial = nullptr; uint32_t group = 0; };
+    struct ClassBuffers {
+        float2* work = nullptr;
+        float* power = nullptr;
+        double* partial = nullptr;
+        uint32_t group = 0;                 // templates per launch
+        uint32_t capacity = 0;              // templates the buffers hold
+        uint32_t partial_per_template = 0;  // pass-1 partial sums per template
+    };
     std::map<uint32_t, ClassBuffers> classes;
     uint32_t max_templates = 0, capacity = 0;
     std::vector<void*> allocations;
@@ -501,9 +509,11 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
         const LengthPlan& lp = kv.second;
         brp_bank::ClassBuffers cb;
         cb.group = std::min(default_group(lp.n), max_templates);
+        cb.capacity = cb.group;
+        cb.partial_per_template = std::max<uint32_t>(lp.blocks1(), lp.M / 64);
         if ((st = b->alloc(&cb.work, size_t(cb.group) * lp.M, "work")) ||
             (st = b->alloc(&cb.power, size_t(cb.group) * lp.M, "power")) ||
-            (st = b->alloc(&cb.partial, size_t(cb.group) * lp.blocks1(), "partial")))
+            (st = b->alloc(&cb.partial, size_t(cb.group) * cb.partial_per_template, "partial")))
             return cleanup(st);
         b->classes[kv.first] = cb;
     }
@@ -564,13 +574,10 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         FusedArgs a{};
         a.inputs = b->d_inputs + t;
         a.params = b->d_params + t;
-        a.n = lp.n; a.M = lp.M; a.L1 = lp.L1; a.L2 = lp.L2; a.C = lp.C; a.R = lp.R;
-        a.plan1[0] = lp.plan1.count; a.plan2[0] = lp.plan2.count;
-        for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
-        a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
+        fill_fused_args(a, lp);
         a.work = cb.work; a.work_stride = lp.M;
         a.power = cb.power; a.power_stride = lp.M;
-        a.partial = cb.partial; a.partial_stride = lp.blocks1();
+        a.partial = cb.partial; a.partial_stride = lp.blocks1();  // per template, within partial_per_template
         a.mean = b->d_mean + t; a.status = b->d_status + t; a.counts = b->d_counts + t;
         a.cands = b->d_cands + size_t(t) * b->capacity;
         a.capacity = b->capacity;
@@ -683,6 +690,54 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     if (dst_off[count] > out_cap) return b->fail(BRP_E_RESULT, "candidate output buffer too small");
     if (bad) return b->fail(BRP_E_RESULT, "GPU invalid resample index or candidate overflow; no valid result");
     return BRP_OK;
+}
+
+extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group) {
+    if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    auto it = b->plans.find(n);
+    if (it == b->plans.end()) return b->fail(BRP_E_ARGUMENT, "no series of that length");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    if ((st = b->cuda(cudaStreamSynchronize(b->stream), "bank configure"))) return st;
+    LengthPlan lp;
+    std::string e = make_length_plan(n, lp, b->stream, pass1, pass2);
+    if (!e.empty()) { free_length_plan(lp); return b->fail(BRP_E_ARGUMENT, e); }
+    if (!lp.fused) { free_length_plan(lp); return b->fail(BRP_E_ARGUMENT, "no fused plan for that configuration"); }
+    brp_bank::ClassBuffers& cb = b->classes.at(n);
+    const uint32_t g = group ? std::min(group, b->max_templates) : cb.group;
+    if (g > cb.capacity || lp.blocks1() > cb.partial_per_template) {
+        // grow the class buffers
+        brp_bank::ClassBuffers nb;
+        nb.capacity = std::max(g, cb.capacity);
+        nb.partial_per_template = std::max(lp.blocks1(), cb.partial_per_template);
+        if ((st = b->alloc(&nb.work, size_t(nb.capacity) * lp.M, "work")) ||
+            (st = b->alloc(&nb.power, size_t(nb.capacity) * lp.M, "power")) ||
+            (st = b->alloc(&nb.partial, size_t(nb.capacity) * nb.partial_per_template, "partial"))) {
+            free_length_plan(lp);
+            return st;
+        }
+        cb.work = nb.work; cb.power = nb.power; cb.partial = nb.partial;
+        cb.capacity = nb.capacity; cb.partial_per_template = nb.partial_per_template;
+    }
+    cb.group = g;
+    free_length_plan(it->second);
+    it->second = lp;
+    b->graph_key.clear();
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* kinds, uint32_t cap) {
+    uint32_t k = 0;
+    for (int kind = 1; kind <= 2; ++kind)
+        for (auto& f : kind == 1 ? fast_pass1_configs() : fast_pass2_configs()) {
+            if (k < cap) {
+                if (ids) ids[k] = f.id;
+                if (lengths) lengths[k] = f.L;
+                if (kinds) kinds[k] = uint32_t(kind);
+            }
+            ++k;
+        }
+    return int(k);
 }
 
 extern "C" int brp_cuda_bank_launch(brp_bank* b) {

@@ -16,6 +16,8 @@ struct RadixPlanHost {
 };
 RadixPlanHost radix_plan(uint32_t length);
 
+struct FastPass;
+
 // Tables of one FFT length class, all FP64-generated and rounded once to FP32.
 //   tw1[L1], tw2[L2]       : W_L^e for the two shared-memory passes
 //   fs_hi/fs_lo (split 2^11): W_M^e, e < M (four-step twiddles)
@@ -31,6 +33,9 @@ struct LengthPlan {
     uint32_t maxe = 16;        // elements per thread held during a shared-memory pass
     uint32_t harm_tile = 2048; // harmonic kernel: trial bins per CTA
     RadixPlanHost plan1, plan2, planB;
+    const FastPass* fp1 = nullptr;  // compiled pass 1 / pass 2 (nullptr: generic kernels)
+    const FastPass* fp2 = nullptr;
+    const float2 *ptw1 = nullptr, *ptw2 = nullptr;
     float2* d_tables = nullptr;
     size_t tables_bytes = 0;
     const float2 *tw1 = nullptr, *tw2 = nullptr, *fs_hi = nullptr, *fs_lo = nullptr, *rl_hi = nullptr,
@@ -41,20 +46,40 @@ struct LengthPlan {
     size_t smem2() const;
 };
 // Chooses the decomposition for length n and uploads its tables.  Returns an
-// error message or empty.
-std::string make_length_plan(uint32_t n, LengthPlan& plan, cudaStream_t stream);
+// error message or empty.  fast1/fast2 (optional) force compiled pass
+// configurations by id (0: default choice, -1: generic kernels).
+std::string make_length_plan(uint32_t n, LengthPlan& plan, cudaStream_t stream, int fast1 = 0, int fast2 = 0);
 void free_length_plan(LengthPlan& plan);
 
 constexpr uint32_t kSplitLog2 = 11;
 
 // Device views passed to the fused kernels.  Per-template arrays are indexed
 // by blockIdx.y (the template within the launch).
+struct FusedArgs;
+// A compiled specialisation of pass 1 (L = L1, group = columns per CTA) or
+// pass 2 (L = L2, group = row pairs per CTA) with its radix sequence and the
+// size of its per-pass twiddle table.
+struct FastPass {
+    int id = 0;
+    uint32_t L = 0, group = 0, threads = 0;
+    size_t smem = 0;
+    void (*launch)(const FusedArgs&, uint32_t blocks, uint32_t count, cudaStream_t) = nullptr;
+    cudaError_t (*attr)() = nullptr;
+    RadixPlanHost plan;
+    int table = 0;
+};
+const std::vector<FastPass>& fast_pass1_configs();
+const std::vector<FastPass>& fast_pass2_configs();
+size_t harmonic_fast_smem();
+cudaError_t set_harmonic_fast_attributes();
+
 struct FusedArgs {
     const float* const* inputs;  // per template: series (unpadded floats)
     const brp_params* params;    // per template
     uint32_t n, M, L1, L2, C, R;
     int plan1[7], plan2[7];      // count followed by radices
     const float2 *tw1, *tw2, *fs_hi, *fs_lo, *rl_hi, *rl_lo;
+    const float2 *ptw1, *ptw2;  // per-pass twiddle tables of the compiled passes
     float2* work;     // per template: M complex (four-step intermediate)
     size_t work_stride;
     float* power;     // per template: M floats (P[k] = |X_k|^2 / n, P[0] = 0)
@@ -78,6 +103,9 @@ void launch_fused_pass1(const FusedArgs& a, const LengthPlan& lp, uint32_t count
 void launch_fused_pass2(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s);
 void launch_fused_harmonic(const FusedArgs& a, const LengthPlan& lp, uint32_t count, uint32_t max_span,
                            cudaStream_t s);
+void launch_harmonic_fast(const FusedArgs& a, uint32_t count, uint32_t max_span, cudaStream_t s);
+// Fills the FFT description and tables of lp into a.
+void fill_fused_args(FusedArgs& a, const LengthPlan& lp);
 
 // Step-by-step pipeline (one template; buffers sized for the length class).
 struct PlainArgs {

@@ -1,5 +1,6 @@
 #!/bin/sh
-# Builds libbrp_cuda.so in this directory's parent (the package root) for sm_100a.
+# Builds libbrp_cuda.so (the package's CUDA backend) for sm_100a.
+# Usage: build.sh [output path]   (default: the package root)
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=${1:-$HERE/../libbrp_cuda.so}
@@ -7,9 +8,15 @@ NVCC=${NVCC:-nvcc}
 TMP=$(mktemp -d)
 trap 'rm -rf "$TMP"' EXIT
 FLAGS="-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 -Xcompiler -fPIC,-ffp-contract=off"
-for f in api plan fused_kernels plain_kernels; do
+PIDS=""
+for f in api plan fused_kernels fused_fast harmonic_fast plain_kernels; do
   $NVCC $FLAGS -c "$HERE/$f.cu" -o "$TMP/$f.o" &
+  PIDS="$PIDS $!"
 done
 g++ -std=c++17 -O2 -fPIC -ffp-contract=off -Wall -Wextra -c "$HERE/host.cpp" -o "$TMP/host.o" &
-wait
-$NVCC -shared -gencode arch=compute_100a,code=sm_100a -o "$OUT" "$TMP"/*.o
+PIDS="$PIDS $!"
+FAIL=0
+for p in $PIDS; do wait "$p" || FAIL=1; done
+[ "$FAIL" = 0 ] || { echo "build.sh: compilation failed" >&2; exit 1; }
+$NVCC -shared -gencode arch=compute_100a,code=sm_100a -o "$OUT.tmp" "$TMP"/*.o
+mv "$OUT.tmp" "$OUT"

@@ -1,0 +1,402 @@
+// Compile-time specialisations of the fused pass 1 and pass 2 kernels (see
+// fused_kernels.cu for the algorithm).  Sequence length, radix sequence,
+// sequences per CTA and thread count are template parameters, so every index
+// computation of the shared-memory Stockham passes folds to shifts and
+// immediate offsets, and each thread holds exactly one butterfly's inputs per
+// pass in registers.  Twiddles of a pass with span Ns and radix R come from a
+// per-pass table tw[k * RS + r - 1] = W_{Ns R}^{r k} (RS = R rounded up to even,
+// so pairs load as one 16-byte access).
+//
+// Resampling uses an instruction-lean form of the reference arithmetic that is
+// bit-identical to it (src/science.cpp:20-40, :80):
+//  * float(i) for i < 2^23 from the exponent trick 0x4B000000 | i;
+//  * the table index int(x) for x in [0.5, 64.5] and float(int(x)) from one
+//    add rounded toward -inf to 2^23 (its low mantissa bits are floor(x));
+//  * (int)((double)index + 0.5) as trunc(fl_toward_zero(index + 0.5)): with
+//    every integer below 2^24 representable, rounding toward zero never crosses
+//    an integer, so truncating the rounded sum equals truncating the exact one.
+// The reference-order function brp_resample_index (resample_math.h) remains the
+// definition; tests compare both against the CPU resampler bit for bit.
+#include "brp_internal.h"
+#include "fft_device.cuh"
+#include "resample_math.h"
+
+namespace brp {
+
+__constant__ uint32_t c_fast_lut_bits[130] = BRP_LUT_BITS;
+
+namespace {
+
+__host__ __device__ constexpr int ct_stride(int L, int G) {
+    int base = L + L / 16;
+    int want = (G >= 16) ? 1 : 16 / G;
+    int pad = ((want - base) % 16 + 16) % 16;
+    return base + pad;
+}
+
+template <int R> struct TwStride { static constexpr int value = (R + 1) & ~1; };
+
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
+__device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ tw) {
+    constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
+    constexpr int RS = TwStride<R>::value;
+    float2 v[PER][R];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int b = threadIdx.x + q * THREADS;
+        if (TOTAL % THREADS == 0 || b < TOTAL) {
+            const int c = b / NBF, j = b - c * NBF;
+            const float2* src = buf + c * STRIDE;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[q][r] = src[smem_pos(j + r * NBF)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int b = threadIdx.x + q * THREADS;
+        if (TOTAL % THREADS == 0 || b < TOTAL) {
+            const int c = b / NBF, j = b - c * NBF;
+            const int k = j % Ns;
+            if constexpr (Ns > 1) {
+                const float4* w4 = reinterpret_cast<const float4*>(tw + k * RS);
+#pragma unroll
+                for (int r = 1; r < R; r += 2) {
+                    const float4 w = __ldg(w4 + (r - 1) / 2);
+                    v[q][r] = cmul(v[q][r], make_float2(w.x, w.y));
+                    if (r + 1 < R) v[q][r + 1] = cmul(v[q][r + 1], make_float2(w.z, w.w));
+                }
+            }
+            dft<R>(v[q]);
+            float2* dst = buf + c * STRIDE;
+            const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[smem_pos(base + r * Ns)] = v[q][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
+__device__ __forceinline__ void ct_fft(float2* buf, const float2* __restrict__ tw) {
+    ct_pass<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw);
+    if constexpr (sizeof...(Rest) > 0)
+        ct_fft<L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R>::value : 0));
+}
+
+// Number of float2 entries of the per-pass twiddle table of a radix sequence.
+template <int Ns, int R, int... Rest>
+__host__ __device__ constexpr int ct_table_size() {
+    int here = Ns > 1 ? Ns * TwStride<R>::value : 0;
+    if constexpr (sizeof...(Rest) > 0) return here + ct_table_size<Ns * R, Rest...>();
+    else return here;
+}
+
+// ---- bit-identical lean resampling index (see the file comment) ----
+__device__ __forceinline__ float u2f_exact(uint32_t i) {
+    return i < (1u << 23) ? __fsub_rn(__int_as_float(0x4B000000 | int(i)), 8388608.0f) : __uint2float_rn(i);
+}
+
+template <bool FMA>
+__device__ __forceinline__ int lean_index(uint32_t i, const brp_resample_consts& p) {
+    const float fi = u2f_exact(i);
+    const float t = __fmul_rn(fi, p.dt);
+    const float ph = FMA ? __fmaf_rn(p.omega, t, p.psi) : __fadd_rn(__fmul_rn(p.omega, t), p.psi);
+    const float y = __fmul_rn(BRP_INV_TWO_PI_F, ph);
+    float xt = __fsub_rn(y, truncf(y));
+    if (xt < 0.f) xt = __fadd_rn(xt, 1.0f);
+    const float x64 = FMA ? __fmaf_rn(xt, 64.0f, 0.5f) : __fadd_rn(__fmul_rn(xt, 64.0f), 0.5f);
+    const float mg = __fadd_rd(x64, 8388608.0f);
+    const int li = __float_as_int(mg) - 0x4B000000;
+    const float fli = __fsub_rn(mg, 8388608.0f);
+    const float s = __uint_as_float(c_fast_lut_bits[2 * li]), c = __uint_as_float(c_fast_lut_bits[2 * li + 1]);
+    float sn, off;
+    if (FMA) {
+        const float d = __fmul_rn(BRP_TWO_PI_F, __fmaf_rn(-fli, 0.015625f, xt));
+        const float d2 = __fmul_rn(__fmul_rn(0.5f, d), d);
+        sn = __fmaf_rn(-d2, s, __fmaf_rn(d, c, s));
+        off = __fmaf_rn(__fmul_rn(p.tau, sn), p.step_inv, -p.s0);
+    } else {
+        const float d = __fmul_rn(BRP_TWO_PI_F, __fsub_rn(xt, __fmul_rn(0.015625f, fli)));
+        const float d2 = __fmul_rn(d, __fmul_rn(0.5f, d));
+        sn = __fsub_rn(__fadd_rn(s, __fmul_rn(d, c)), __fmul_rn(d2, s));
+        off = __fsub_rn(__fmul_rn(__fmul_rn(p.tau, sn), p.step_inv), p.s0);
+    }
+    const float index = __fsub_rn(fi, off);
+    return __float2int_rz(__fadd_rz(index, 0.5f));
+}
+
+__device__ __forceinline__ brp_resample_consts consts_of(const brp_params& p) {
+    brp_resample_consts c;
+    c.tau = p.tau; c.omega = p.omega; c.psi = p.psi; c.dt = p.dt; c.step_inv = p.step_inv; c.s0 = p.s0;
+    c.flags = p.flags;
+    return c;
+}
+
+template <int THREADS>
+__device__ __forceinline__ double block_sum_d(double v, double* scratch) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double r = 0;
+    if (warp == 0) {
+        r = lane < THREADS / 32 ? scratch[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+
+// Gathers this CTA's samples (rows n1 < L1, 2C consecutive reals per row) into
+// shared memory; returns the sum of the samples (FP32 per thread, at most a few
+// dozen samples, then FP64 across threads).  Thread t always handles the same
+// position rem = t % 2C of its rows, so the sample index, its float value and
+// the shared-memory address advance by constants.
+template <int L1, int C, int THREADS, int STRIDE, int MODE>
+__device__ __forceinline__ double gather(float* smf, const float* __restrict__ in, const brp_params& P,
+                                         uint32_t L2, uint32_t c0, float* raw, bool& oob) {
+    constexpr int ROW = 2 * C, TOTAL = L1 * ROW, PER = TOTAL / THREADS, ROWS_STEP = THREADS / ROW;
+    static_assert(TOTAL % THREADS == 0 && THREADS % ROW == 0, "gather must tile the CTA");
+    static_assert(ROWS_STEP % 16 == 0, "row step must keep the shared-memory padding periodic");
+    const brp_resample_consts rc = consts_of(P);
+    const uint32_t steps = P.steps, unpadded = P.unpadded;
+    const int rem = threadIdx.x % ROW, n1_0 = threadIdx.x / ROW;
+    const uint32_t istep = 2u * L2 * ROWS_STEP;
+    uint32_t i = 2u * (L2 * uint32_t(n1_0) + c0) + uint32_t(rem);
+    float* dst = smf + 2 * ((rem >> 1) * STRIDE + smem_pos(n1_0)) + (rem & 1);
+    constexpr int DSTEP = 2 * (ROWS_STEP + ROWS_STEP / 16);
+    float sum = 0.f;
+#pragma unroll 4
+    for (int q = 0; q < PER; ++q, i += istep, dst += DSTEP) {
+        float v = 0.f;
+        if (i < steps) {
+            int j;
+            if (MODE == 2) j = brp_resample_index_fp64(i, rc);
+            else j = lean_index<MODE == 1>(i, rc);
+            if (uint32_t(j) < unpadded) v = __ldg(in + j);
+            else oob = true;
+            if (raw) raw[i] = v;
+        }
+        sum += v;
+        *dst = v;
+    }
+    return double(sum);
+}
+
+template <int L1, int C, int THREADS, int MINB, int... Rs>
+__global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
+    constexpr int STRIDE = ct_stride(L1, C);
+    extern __shared__ float2 sm[];
+    __shared__ double red[THREADS / 32];
+    const int g = blockIdx.y;
+    const brp_params& P = a.params[g];
+    const float* __restrict__ in = a.inputs[g];
+    const uint32_t L2 = a.L2, c0 = blockIdx.x * C;
+    float* raw = (g == a.snap) ? a.snap_raw : nullptr;
+    float* smf = reinterpret_cast<float*>(sm);
+    bool oob = false;
+    double sum;
+    if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(smf, in, P, L2, c0, raw, oob);
+    else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(smf, in, P, L2, c0, raw, oob);
+    else sum = gather<L1, C, THREADS, STRIDE, 0>(smf, in, P, L2, c0, raw, oob);
+    if (oob) atomicOr(a.status + g, BRP_STATUS_RESAMPLE_OOB);
+    const double tot = block_sum_d<THREADS>(sum, red);
+    if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
+    __syncthreads();
+
+    ct_fft<L1, STRIDE, C, THREADS, 1, Rs...>(sm, a.ptw1);
+
+    float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < L1 * C; idx += THREADS) {
+        const int k1 = idx / C, c = idx % C;
+        float2 y = sm[c * STRIDE + smem_pos(k1)];
+        const uint32_t e = (c0 + uint32_t(c)) * uint32_t(k1);
+        y = cmul(y, twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, e));
+        T[size_t(k1) * L2 + c0 + c] = y;
+    }
+}
+
+__device__ __forceinline__ uint32_t mod_n(uint64_t x, uint32_t n) {
+    if ((n & (n - 1)) == 0) return uint32_t(x & (n - 1));
+    const uint32_t s = __ffs(n) - 1;
+    return uint32_t((((x >> s) % 3ull) << s) | (x & ((1ull << s) - 1)));
+}
+
+__device__ __forceinline__ float2 real_bin(float2 zk, float2 zm, float2 w, float2 pad) {
+    const float2 s = make_float2(zk.x + zm.x, zk.y - zm.y);
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+    const float2 t = cmul(w, d);
+    return make_float2(0.5f * (s.x + t.y) + pad.x, 0.5f * (s.y - t.x) + pad.y);
+}
+
+template <int L2, int R, int THREADS, int MINB, int... Rs>
+__global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
+    constexpr int SEQ = 2 * R, STRIDE = ct_stride(L2, R);
+    extern __shared__ float2 sm[];
+    __shared__ double red[THREADS / 32];
+    __shared__ float s_mean;
+    const int g = blockIdx.y, q = blockIdx.x;
+    const brp_params& P = a.params[g];
+    const uint32_t L1 = a.L1, n = a.n, M = a.M, steps = P.steps;
+    const float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
+
+    // rows [0, R): qR + r; rows [R, 2R): L1 - (qR + r), row L1/2 in place of row 0's mirror
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < SEQ * L2 / 2; idx += THREADS) {
+        const int rr = idx / (L2 / 2), k2 = 2 * (idx % (L2 / 2));
+        uint32_t row;
+        if (rr < R) row = q * R + rr;
+        else {
+            const uint32_t ar = q * R + (rr - R);
+            row = ar == 0 ? L1 / 2 : L1 - ar;
+        }
+        const float4 x = __ldg(reinterpret_cast<const float4*>(T + size_t(row) * L2 + k2));
+        sm[rr * STRIDE + smem_pos(k2)] = make_float2(x.x, x.y);
+        sm[rr * STRIDE + smem_pos(k2 + 1)] = make_float2(x.z, x.w);
+    }
+    double part = 0;
+    const double* pp = a.partial + size_t(g) * a.partial_stride;
+    for (uint32_t i = threadIdx.x; i < a.partial_stride; i += THREADS) part += pp[i];
+    const double tot = block_sum_d<THREADS>(part, red);
+    if (threadIdx.x == 0) {
+        const float mean = float(tot / double(steps));
+        s_mean = mean;
+        if (q == 0) a.mean[g] = mean;
+    }
+    __syncthreads();
+    const float mean = s_mean;
+
+    ct_fft<L2, STRIDE, SEQ, THREADS, 1, Rs...>(sm, a.ptw2);
+
+    float* __restrict__ Pw = a.power + size_t(g) * a.power_stride;
+    float2* fft = (g == a.snap) ? a.snap_fft : nullptr;
+    const bool pow2 = (n & (n - 1)) == 0;
+    const float inv_n = 1.0f / float(n), fn = float(n);
+    const bool a_odd = steps & 1u;
+    const float pad0 = float(n - steps) * mean;
+
+#pragma unroll 2
+    for (int idx = threadIdx.x; idx < R * L2; idx += THREADS) {
+        const int r = idx % R, k2 = idx / R;
+        const uint32_t arow = q * R + r;
+        if (arow == 0) {
+#pragma unroll
+            for (int which = 0; which < 2; ++which) {
+                const int rr = which == 0 ? 0 : R;
+                const uint32_t k = which == 0 ? L1 * k2 : L1 / 2 + L1 * k2;
+                const int m2 = which == 0 ? (L2 - k2) % L2 : L2 - 1 - k2;
+                const float2 zk = sm[rr * STRIDE + smem_pos(k2)], zm = sm[rr * STRIDE + smem_pos(m2)];
+                float2 X;
+                if (k == 0) {
+                    X = make_float2(zk.x + zk.y + pad0, 0.f);
+                    if (fft) fft[M] = make_float2(zk.x - zk.y - (a_odd ? mean : 0.f), 0.f);
+                    Pw[0] = 0.f;
+                } else {
+                    float sv, cv;
+                    sincospif(float(k) / fn, &sv, &cv);
+                    const float2 wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+                    const float2 G = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
+                    const float f = __fdividef(-0.5f * mean, sv);
+                    X = real_bin(zk, zm, twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, k), make_float2(G.x * f, G.y * f));
+                    const float pw = X.x * X.x + X.y * X.y;
+                    Pw[k] = pow2 ? pw * inv_n : pw / fn;
+                }
+                if (fft) fft[k] = X;
+            }
+        } else {
+            const uint32_t brow = L1 - arow;
+            const uint32_t k = arow + L1 * k2;
+            const uint32_t km = brow + L1 * uint32_t(L2 - 1 - k2);
+            const float2 zk = sm[r * STRIDE + smem_pos(k2)], zm = sm[(R + r) * STRIDE + smem_pos(L2 - 1 - k2)];
+            float sv, cv;
+            sincospif(float(k) / fn, &sv, &cv);
+            const float2 w = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, k);
+            const float2 wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+            const float2 wm = make_float2(-w.x, w.y);
+            const float2 wam = a_odd ? make_float2(-wa.x, wa.y) : make_float2(wa.x, -wa.y);
+            const float2 G1 = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
+            const float2 G2 = cmul(make_float2(1.f - wam.x, -wam.y), make_float2(cv, -sv));
+            const float hm = -0.5f * mean;
+            const float f1 = __fdividef(hm, sv), f2 = __fdividef(hm, cv);
+            const float2 X1 = real_bin(zk, zm, w, make_float2(G1.x * f1, G1.y * f1));
+            const float2 X2 = real_bin(zm, zk, wm, make_float2(G2.x * f2, G2.y * f2));
+            const float p1 = X1.x * X1.x + X1.y * X1.y, p2 = X2.x * X2.x + X2.y * X2.y;
+            Pw[k] = pow2 ? p1 * inv_n : p1 / fn;
+            Pw[km] = pow2 ? p2 * inv_n : p2 / fn;
+            if (fft) { fft[k] = X1; fft[km] = X2; }
+        }
+    }
+}
+
+// ---- registry of compiled configurations ----
+template <int L1, int C, int THREADS, int MINB, int... Rs>
+struct P1 {
+    static constexpr int smem = C * ct_stride(L1, C) * 8;
+    static void launch(const FusedArgs& a, uint32_t blocks, uint32_t count, cudaStream_t s) {
+        pass1_fast<L1, C, THREADS, MINB, Rs...><<<dim3(blocks, count), THREADS, smem, s>>>(a);
+    }
+    static cudaError_t attr() {
+        return cudaFuncSetAttribute(pass1_fast<L1, C, THREADS, MINB, Rs...>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    static FastPass info(int id) {
+        FastPass f;
+        f.id = id; f.L = L1; f.group = C; f.threads = THREADS; f.smem = smem; f.launch = &launch; f.attr = &attr;
+        int r[] = {Rs...};
+        f.plan.count = int(sizeof...(Rs));
+        for (int i = 0; i < f.plan.count; ++i) f.plan.radix[i] = r[i];
+        f.table = ct_table_size<1, Rs...>();
+        return f;
+    }
+};
+template <int L2, int R, int THREADS, int MINB, int... Rs>
+struct P2 {
+    static constexpr int smem = 2 * R * ct_stride(L2, R) * 8;
+    static void launch(const FusedArgs& a, uint32_t blocks, uint32_t count, cudaStream_t s) {
+        pass2_fast<L2, R, THREADS, MINB, Rs...><<<dim3(blocks, count), THREADS, smem, s>>>(a);
+    }
+    static cudaError_t attr() {
+        return cudaFuncSetAttribute(pass2_fast<L2, R, THREADS, MINB, Rs...>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    static FastPass info(int id) {
+        FastPass f;
+        f.id = id; f.L = L2; f.group = R; f.threads = THREADS; f.smem = smem; f.launch = &launch; f.attr = &attr;
+        int r[] = {Rs...};
+        f.plan.count = int(sizeof...(Rs));
+        for (int i = 0; i < f.plan.count; ++i) f.plan.radix[i] = r[i];
+        f.table = ct_table_size<1, Rs...>();
+        return f;
+    }
+};
+
+}  // namespace
+
+const std::vector<FastPass>& fast_pass1_configs() {
+    static const std::vector<FastPass> v = {
+        P1<2048, 4, 512, 2, 16, 16, 8>::info(101),
+        P1<2048, 2, 256, 4, 16, 16, 8>::info(102),
+        P1<1024, 4, 256, 4, 16, 8, 8>::info(103),
+        P1<1024, 8, 512, 2, 16, 8, 8>::info(104),
+        P1<1536, 4, 384, 2, 8, 8, 8, 3>::info(105),
+        P1<3072, 2, 384, 2, 16, 16, 4, 3>::info(106),
+        P1<512, 8, 256, 4, 8, 8, 8>::info(107),
+    };
+    return v;
+}
+
+const std::vector<FastPass>& fast_pass2_configs() {
+    static const std::vector<FastPass> v = {
+        P2<1024, 2, 256, 4, 16, 8, 8>::info(201),
+        P2<1024, 4, 512, 2, 16, 8, 8>::info(202),
+        P2<512, 4, 256, 4, 8, 8, 8>::info(203),
+        P2<2048, 2, 512, 2, 16, 16, 8>::info(204),
+        P2<512, 8, 512, 2, 8, 8, 8>::info(205),
+    };
+    return v;
+}
+
+}  // namespace brp

@@ -378,10 +378,12 @@ cudaError_t set_fused_attributes(size_t max_dynamic_smem) {
 }
 
 void launch_fused_pass1(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s) {
+    if (lp.fp1) { lp.fp1->launch(a, lp.blocks1(), count, s); return; }
     if (lp.maxe <= 16) launch_p1<16>(a, lp, count, s);
     else launch_p1<24>(a, lp, count, s);
 }
 void launch_fused_pass2(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s) {
+    if (lp.fp2) { lp.fp2->launch(a, lp.blocks2(), count, s); return; }
     if (lp.maxe <= 16) launch_p2<16>(a, lp, count, s);
     else launch_p2<24>(a, lp, count, s);
 }
@@ -389,10 +391,19 @@ void launch_fused_pass2(const FusedArgs& a, const LengthPlan& lp, uint32_t count
 // top fundamental bin of level h may own trial bins up to harmonic + 2^(h-1).
 void launch_fused_harmonic(const FusedArgs& a, const LengthPlan& lp, uint32_t count, uint32_t max_span,
                            cudaStream_t s) {
+    if (lp.fused) { launch_harmonic_fast(a, count, max_span, s); return; }
     constexpr int T = 2048;
     uint32_t tiles = (max_span + T - 1) / T;
     if (!tiles) tiles = 1;
     harmonic_kernel<T, 256><<<dim3(tiles, count), 256, 0, s>>>(a);
+}
+
+void fill_fused_args(FusedArgs& a, const LengthPlan& lp) {
+    a.n = lp.n; a.M = lp.M; a.L1 = lp.L1; a.L2 = lp.L2; a.C = lp.C; a.R = lp.R;
+    a.plan1[0] = lp.plan1.count; a.plan2[0] = lp.plan2.count;
+    for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
+    a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
+    a.ptw1 = lp.ptw1; a.ptw2 = lp.ptw2;
 }
 
 }  // namespace brp

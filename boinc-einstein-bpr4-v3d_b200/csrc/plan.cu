@@ -39,7 +39,34 @@ static void fill_twiddles(float2* out, uint32_t count, uint64_t period, uint64_t
 
 size_t plan_smem_limit() { return 110 * 1024; }
 
-std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
+static const FastPass* find_fast(const std::vector<FastPass>& v, uint32_t L, int want) {
+    if (want < 0) return nullptr;
+    for (auto& f : v)
+        if (f.L == L && (want == 0 || f.id == want)) return &f;
+    return nullptr;
+}
+
+// Per-pass twiddle table of a radix sequence: pass p (span Ns = product of the
+// earlier radices, radix R) holds W_{Ns R}^{r k} at [k * RS + r - 1], RS = R
+// rounded up to even; the first pass (Ns = 1) needs none.
+static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
+    uint64_t Ns = 1;
+    size_t at = 0;
+    for (int p = 0; p < plan.count; ++p) {
+        const uint64_t R = plan.radix[p], RS = (R + 1) & ~uint64_t(1);
+        if (Ns > 1)
+            for (uint64_t k = 0; k < Ns; ++k)
+                for (uint64_t r = 0; r < RS; ++r) {
+                    const uint64_t e = (r + 1 < R) ? ((r + 1) * k) % (Ns * R) : 0;
+                    const double ang = -2.0 * M_PI * (double(e) / double(Ns * R));
+                    out[at + k * RS + r] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
+                }
+        if (Ns > 1) at += Ns * RS;
+        Ns *= R;
+    }
+}
+
+std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream, int fast1, int fast2) {
     const bool radix3 = !is_pow2(n);
     if (n < 64 || n > 3u * (1u << 22) || (radix3 && !(n % 3 == 0 && is_pow2(n / 3))))
         return "series length must be 2^k or 3*2^k in 64..3*2^22";
@@ -51,7 +78,23 @@ std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
     lp.planB = radix_plan(lp.B);
     // Fused two-pass decomposition for M >= 4096: L2 = 2^min(10, a/2) (a = log2 of
     // the power-of-two part of M), L1 = M / L2 <= 4096.
-    if (lp.M >= 4096) {
+    // Compiled two-pass decomposition when one exists (rows of 1024 preferred).
+    if (lp.M >= 4096 && fast1 >= 0 && fast2 >= 0) {
+        for (uint32_t l2 : {1024u, 512u, 2048u, 256u}) {
+            if (lp.M % l2 || lp.M / l2 > 4096) continue;
+            const FastPass* f1 = find_fast(fast_pass1_configs(), lp.M / l2, fast1);
+            const FastPass* f2 = find_fast(fast_pass2_configs(), l2, fast2);
+            if (!f1 || !f2 || l2 % f1->group || (lp.M / l2) % (2 * f2->group)) continue;
+            lp.fp1 = f1; lp.fp2 = f2;
+            lp.L1 = lp.M / l2; lp.L2 = l2; lp.C = f1->group; lp.R = f2->group;
+            lp.plan1 = f1->plan; lp.plan2 = f2->plan;
+            lp.fused = true;
+            if (f1->attr() != cudaSuccess || f2->attr() != cudaSuccess)
+                return "cannot enable the shared memory of the compiled fused kernels";
+            break;
+        }
+    }
+    if (lp.M >= 4096 && !lp.fp1) {
         uint32_t a = ilog2(lp.B);
         uint32_t l2 = 1u << std::min<uint32_t>(10, a / 2);
         while (lp.M / l2 > 4096) l2 <<= 1;
@@ -73,13 +116,17 @@ std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
         if (lp.fused && set_fused_attributes(std::max(lp.smem1(), lp.smem2())) != cudaSuccess)
             return "cannot enable the shared memory of the fused kernels";
     }
+    if (lp.fused && set_harmonic_fast_attributes() != cudaSuccess)
+        return "cannot enable the shared memory of the harmonic kernel";
     // Tables: tw1[L1] tw2[L2] fs_hi[ceil(M/2048)] fs_lo[2048] rl_hi[ceil(n/2048)] rl_lo[2048] twb[B]
+    // ptw1 ptw2 (per-pass tables of the compiled passes); each block 16-byte aligned.
     const uint32_t split = 1u << kSplitLog2;
     const uint32_t fs_hi_n = (lp.M + split - 1) / split, rl_hi_n = (n + split - 1) / split;
-    std::vector<size_t> off(8, 0);
+    std::vector<size_t> off(10, 0);
     size_t total = 0;
-    const uint32_t counts[7] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, lp.B};
-    for (int i = 0; i < 7; ++i) { off[i] = total; total += counts[i]; }
+    const uint32_t counts[9] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, lp.B,
+                                uint32_t(lp.fp1 ? lp.fp1->table : 0), uint32_t(lp.fp2 ? lp.fp2->table : 0)};
+    for (int i = 0; i < 9; ++i) { off[i] = total; total += (counts[i] + 1) & ~1u; }
     std::vector<float2> host(total);
     if (lp.L1) fill_twiddles(host.data() + off[0], lp.L1, lp.L1, 0, 1);
     if (lp.L2) fill_twiddles(host.data() + off[1], lp.L2, lp.L2, 0, 1);
@@ -88,6 +135,8 @@ std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
     fill_twiddles(host.data() + off[4], rl_hi_n, n, 0, split);
     fill_twiddles(host.data() + off[5], split, n, 0, 1);
     fill_twiddles(host.data() + off[6], lp.B, lp.B, 0, 1);
+    if (lp.fp1) fill_pass_tables(host.data() + off[7], lp.plan1);
+    if (lp.fp2) fill_pass_tables(host.data() + off[8], lp.plan2);
     lp.tables_bytes = total * sizeof(float2);
     if (cudaMalloc(&lp.d_tables, lp.tables_bytes) != cudaSuccess) return "cudaMalloc of twiddle tables failed";
     if (cudaMemcpyAsync(lp.d_tables, host.data(), lp.tables_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
@@ -100,6 +149,8 @@ std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream) {
     lp.rl_hi = lp.d_tables + off[4];
     lp.rl_lo = lp.d_tables + off[5];
     lp.twb = lp.d_tables + off[6];
+    lp.ptw1 = lp.d_tables + off[7];
+    lp.ptw2 = lp.d_tables + off[8];
     return "";
 }
 

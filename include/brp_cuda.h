@@ -74,6 +74,8 @@ typedef struct brp_options {
     uint32_t batch;     /* 1..64 templates per run (src/vulkan.cpp:121) */
     uint32_t flags;     /* BRP_OPT_* */
     int32_t device;     /* CUDA device ordinal; -1 = the calling thread's current device */
+    /* reserved[0], reserved[1]: compiled pass-1 / pass-2 configuration ids
+     * (brp_cuda_fast_configs); 0 = default, UINT32_MAX = generic kernels. */
     uint32_t reserved[3];
 } brp_options;
 
@@ -133,6 +135,14 @@ int brp_cuda_bank_set_series(brp_bank* bank, uint32_t series, const float* input
  * out_cap is too small.  Blocks until done. */
 int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count,
                       brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status);
+/* Selects the kernels of one length class: compiled pass-1 / pass-2
+ * configuration ids (0 = default, -1 = generic kernels) and templates per
+ * launch (0 = keep).  Used by the autotuner; the next run re-captures. */
+int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group);
+/* Lists the compiled configurations: ids, sequence length L (pass 1: column
+ * length L1, pass 2: row length L2) and kind (1 = pass 1, 2 = pass 2).
+ * Returns the total count; writes at most cap entries. */
+int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* kinds, uint32_t cap);
 /* Device-only replay of the last brp_cuda_bank_run's graph (no host copies,
  * no wait): the throughput kernel time is measured around this by the caller
  * with events on brp_cuda_bank_stream(). */
