@@ -49,6 +49,11 @@ class Params(ctypes.Structure):
 assert ctypes.sizeof(Params) == 108
 
 
+def as_params(p):
+    """Any 108-byte brp::Params-layout structure as a Params (copied)."""
+    return Params.from_buffer_copy(bytes(p))
+
+
 class Options(ctypes.Structure):
     _fields_ = [("workgroup", ctypes.c_uint32), ("tile", ctypes.c_uint32), ("batch", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("device", ctypes.c_int32), ("reserved", ctypes.c_uint32 * 3)]

@@ -5,7 +5,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import CANDIDATE, BrpError, Params, check, lib, ptr
+from ._lib import CANDIDATE, BrpError, Params, as_params, check, lib, ptr
 
 
 class Bank:
@@ -44,7 +44,7 @@ class Bank:
         """Searches every template; returns (candidates per template, counts, status).
         Raises BrpError when a template overflowed or resampled out of range."""
         count = len(templates)
-        arr = (Params * count)(*templates)
+        arr = (Params * count)(*[as_params(t) for t in templates])
         so = np.zeros(count, np.uint32) if series_of is None else np.ascontiguousarray(series_of, dtype=np.uint32)
         counts = np.zeros(count, np.uint32)
         status = np.zeros(count, np.uint32)

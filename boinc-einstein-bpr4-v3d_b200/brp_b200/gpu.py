@@ -9,7 +9,7 @@ from collections import namedtuple
 
 import numpy as np
 
-from ._lib import CANDIDATE, OPT, BrpError, Options, Params, Timings, check, lib, ptr
+from ._lib import CANDIDATE, OPT, BrpError, Options, Params, Timings, as_params, check, lib, ptr
 
 Snapshot = namedtuple("Snapshot", "resampled power summed fft candidates")
 RunTimings = namedtuple("RunTimings", "wall_ms cpu_ms submit_ms stage_ms template_stage_ms")
@@ -33,6 +33,7 @@ class GPU:
         o.reserved[0] = pass1 & 0xFFFFFFFF  # compiled pass configuration ids (-1: generic kernels)
         o.reserved[1] = pass2 & 0xFFFFFFFF
         ctx = ctypes.c_void_p()
+        params = as_params(params)
         st = L.brp_cuda_create(ctypes.byref(params), ptr(x), x.size, ctypes.byref(o), ctypes.byref(ctx))
         check(st, lambda: L.brp_cuda_last_error(None).decode())
         self._ctx = ctx
@@ -61,7 +62,7 @@ class GPU:
         self.set_templates([p])
 
     def set_templates(self, templates):
-        arr = (Params * len(templates))(*templates)
+        arr = (Params * len(templates))(*[as_params(t) for t in templates])
         check(lib().brp_cuda_set_templates(self._ctx, arr, len(templates)), self._err)
         self._templates = [t.copy() for t in templates]
 

@@ -5,7 +5,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import BANK_CANDIDATE, CANDIDATE, BrpError, Params, lib, ptr
+from ._lib import BANK_CANDIDATE, CANDIDATE, BrpError, Params, as_params, lib, ptr
 
 
 def _err():
@@ -23,7 +23,7 @@ def parameters(n, unpadded, tau, period, psi, dt):
 
 
 def resampling_steps(p):
-    q = p.copy()
+    q = as_params(p)
     st = lib().brp_host_resampling_steps(ctypes.byref(q))
     if st:
         raise BrpError(st, "template produces empty series")
@@ -32,7 +32,7 @@ def resampling_steps(p):
 
 def production(p):
     """src/main.cpp:41: FMA resampling arithmetic (flags 2|4) with the float-sine S0."""
-    q = p.copy()
+    q = as_params(p)
     q.flags = 2 | 4
     q.s0 = np.float32(np.float32(q.tau) * np.sin(np.float32(q.psi))) * np.float32(q.step_inv)
     return resampling_steps(q)
@@ -62,13 +62,13 @@ class Toplist:
             self._t = None
 
     def thresholds(self, p):
-        q = p.copy()
+        q = as_params(p)
         lib().brp_toplist_thresholds(self._t, ctypes.byref(q))
         return q
 
     def retain(self, candidates, period, tau, psi, p):
         c = np.ascontiguousarray(candidates, dtype=CANDIDATE)
-        st = lib().brp_toplist_retain(self._t, ptr(c), c.size, period, tau, psi, ctypes.byref(p))
+        st = lib().brp_toplist_retain(self._t, ptr(c), c.size, period, tau, psi, ctypes.byref(as_params(p)))
         if st:
             raise BrpError(st, "invalid compact candidate")
 

@@ -1,0 +1,69 @@
+"""The C-ABI library loads without a GPU and exports every function that
+include/brp_cuda.h declares; the oracle library exports its C interface."""
+import ctypes
+import os
+import re
+
+import brp_b200 as B
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(brp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_symbols_exported():
+    names = declared(os.path.join(ROOT, "include", "brp_cuda.h"))
+    assert len(names) >= 25
+    lib = ctypes.CDLL(B.build())
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(B.EXPORTS) <= set(names)
+
+
+def test_params_layout_matches_reference():
+    assert ctypes.sizeof(B.Params) == 108
+    assert B.Params.threshold.offset == 56 and B.Params.result_slot.offset == 104
+    assert B.CANDIDATE.itemsize == 16 and B.BANK_CANDIDATE.itemsize == 48
+
+
+def test_errors_without_device_are_reported():
+    # no CUDA device here: creating a context fails with a message, never crashes
+    import numpy as np
+    import pytest
+    p = B.parameters(8192, 8000, 0.1, 600.0, 0.0, 128e-6)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    with pytest.raises(B.BrpError) as e:
+        B.GPU(p, np.zeros(8000, np.float32), 192, 0, 1)
+    assert str(e.value)
+
+
+def test_option_validation_matches_reference():
+    # src/vulkan.cpp:278-284: flag combinations are rejected before any device work
+    import numpy as np
+    import pytest
+    p = B.parameters(8192, 8000, 0.1, 600.0, 0.0, 128e-6)
+    x = np.zeros(8000, np.float32)
+    for kw in (dict(fused_power=True), dict(radix8_store=True), dict(radix8=True, stockham=False),
+               dict(stockham=True, tile=512)):
+        args = dict(workgroup=192, tile=0, batch=1)
+        args.update(kw)
+        with pytest.raises(B.BrpError) as e:
+            B.GPU(p, x, **args)
+        assert e.value.status == 1
+
+
+def test_oracle_library_exports():
+    from oracle import oracle as O
+    L = O.lib()
+    for name in ("oracle_resample", "oracle_harmonic", "oracle_select", "oracle_search_parameters",
+                 "oracle_toplist_retain", "oracle_toplist_final", "oracle_rfft64"):
+        assert hasattr(L, name)
