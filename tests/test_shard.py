@@ -27,7 +27,7 @@ def free_port():
 
 def small_bank():
     from brp_b200 import synth
-    return synth.bank_workload("shard-test", [1 << 16], [11], [1], seed=31, f0=800.0, sigmas=(3.0,))
+    return synth.bank_workload("shard-test", [1 << 16], [11], [1], seed=31, f0=800.0, sigmas=(3.5,))
 
 
 def _worker(rank, world, port, outdir, fail_rank):
