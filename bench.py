@@ -258,7 +258,7 @@ def main():
         from brp_b200 import tune
         bank.set_series(0, x_host)
         res = tune.autotune(bank, my_templates, use_cache=False)
-        plan = {str(n): {k: r[k] for k in ("pass1", "pass2", "group", "ms")} for n, r in res.items()}
+        plan = {str(n): {k: r[k] for k in ("pass1", "pass2", "group", "chains", "ms")} for n, r in res.items()}
         if os.environ.get("BRP_BENCH_VERBOSE"):
             print(json.dumps({"tuning": {str(n): r.get("tried") for n, r in res.items()}}), file=sys.stderr)
     for _ in range(max(args.warmup, 3)):

@@ -81,7 +81,7 @@ EXPORTS = (
     "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_configure", "brp_cuda_fast_configs", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
     "brp_cuda_bank_last_error", "brp_host_parameters", "brp_host_resampling_steps", "brp_host_search_parameters",
     "brp_toplist_create", "brp_toplist_destroy", "brp_toplist_thresholds", "brp_toplist_retain",
-    "brp_toplist_final",
+    "brp_toplist_final", "brp_toplist_fold",
 )
 
 
@@ -118,7 +118,7 @@ def lib():
             L.brp_cuda_bank_set_series.argtypes = [vp, u32, vp]
             L.brp_cuda_bank_run.argtypes = [vp, vp, vp, u32, vp, u64, vp, vp]
             L.brp_cuda_bank_launch.argtypes = [vp]
-            L.brp_cuda_bank_configure.argtypes = [vp, u32, ctypes.c_int32, ctypes.c_int32, u32]
+            L.brp_cuda_bank_configure.argtypes = [vp, u32, ctypes.c_int32, ctypes.c_int32, u32, u32]
             L.brp_cuda_fast_configs.argtypes = [vp, vp, vp, u32]
             L.brp_cuda_bank_profile.argtypes = [vp, vp, vp]
             L.brp_cuda_bank_stream.argtypes = [vp]
@@ -137,6 +137,7 @@ def lib():
             L.brp_toplist_thresholds.argtypes = [vp, P]
             L.brp_toplist_thresholds.restype = None
             L.brp_toplist_retain.argtypes = [vp, vp, u32, ctypes.c_double, ctypes.c_double, ctypes.c_double, P]
+            L.brp_toplist_fold.argtypes = [vp, vp, vp, vp, vp, u32]
             L.brp_toplist_final.argtypes = [vp, vp]
             L.brp_toplist_final.restype = u32
             _lib = L

@@ -65,9 +65,10 @@ class Bank:
             raise e
         return result, counts, status
 
-    def configure(self, n, pass1=0, pass2=0, group=0):
-        """Selects compiled pass configurations and templates per launch for length n."""
-        check(lib().brp_cuda_bank_configure(self._b, n, pass1, pass2, group), self._err)
+    def configure(self, n, pass1=0, pass2=0, group=0, chains=0):
+        """Selects compiled pass configurations, templates per launch and
+        parallel launch chains for length n."""
+        check(lib().brp_cuda_bank_configure(self._b, n, pass1, pass2, group, chains), self._err)
 
     def launch(self):
         """Replays the last run's graph on the device only (no copies, no wait)."""

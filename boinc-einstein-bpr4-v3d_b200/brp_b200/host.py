@@ -72,6 +72,18 @@ class Toplist:
         if st:
             raise BrpError(st, "invalid compact candidate")
 
+    def fold(self, templates, orbits, candidates):
+        """Thresholds + retain for every template in bank order, in one call."""
+        count = len(templates)
+        arr = (Params * count)(*[as_params(t) for t in templates])
+        orb = np.ascontiguousarray(orbits, dtype=np.float64).reshape(count, 3)
+        counts = np.array([len(c) for c in candidates], np.uint32)
+        flat = np.ascontiguousarray(np.concatenate(candidates) if count else np.zeros(0, CANDIDATE), dtype=CANDIDATE)
+        st = lib().brp_toplist_fold(self._t, arr, ptr(orb), ptr(flat), ptr(counts), count)
+        if st:
+            raise BrpError(st, "invalid compact candidate")
+        return self
+
     def final(self):
         out = np.zeros(100, BANK_CANDIDATE)
         n = lib().brp_toplist_final(self._t, ptr(out))

@@ -40,6 +40,8 @@ def gather_candidates(per_template, begin, group=None):
 
 def fold_toplist(toplist, templates, orbits, candidates):
     """Retains every template's candidates in bank order (src/workunit_main.cpp:124)."""
+    if hasattr(toplist, "fold"):
+        return toplist.fold(templates, orbits, candidates)
     for p, orb, c in zip(templates, orbits, candidates):
         q = toplist.thresholds(p)
         toplist.retain(c, orb[0], orb[1], orb[2], q)

@@ -17,8 +17,8 @@ from ._lib import fast_configs
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "brp_b200", "plans.json")
 
 
-def candidates(n, groups=(4, 8, 16)):
-    """(pass1 id, pass2 id, group) triples whose decomposition covers length n."""
+def candidates(n, groups=(4, 8, 16), chains=(1, 2)):
+    """(pass1 id, pass2 id, group, chains) whose decomposition covers length n."""
     M = n // 2
     cfg = fast_configs()
     p1 = [(i, L) for i, L, k in cfg if k == 1]
@@ -28,7 +28,8 @@ def candidates(n, groups=(4, 8, 16)):
         for i2, L2 in p2:
             if L1 * L2 == M:
                 for g in groups:
-                    out.append((i1, i2, g))
+                    for c in chains:
+                        out.append((i1, i2, g, c))
     return out
 
 
@@ -78,7 +79,8 @@ def time_replays(bank, reps, flush):
     return total / reps
 
 
-def autotune(bank, templates, series_of=None, reps=3, groups=(4, 8, 16), cache_path=DEFAULT_CACHE, use_cache=True):
+def autotune(bank, templates, series_of=None, reps=3, groups=(8, 16), chains=(1, 2), cache_path=DEFAULT_CACHE,
+             use_cache=True):
     """Chooses the fastest configuration for every length class of `bank` on
     this workload; leaves the bank configured with it and returns
     {n: {"pass1": id, "pass2": id, "group": g, "ms": t, "tried": [...]}}."""
@@ -93,27 +95,27 @@ def autotune(bank, templates, series_of=None, reps=3, groups=(4, 8, 16), cache_p
         key = "%s|n=%d|templates=%d" % (dev, n, len(templates))
         if use_cache and key in cache:
             c = cache[key]
-            bank.configure(n, c["pass1"], c["pass2"], c["group"])
+            bank.configure(n, c["pass1"], c["pass2"], c["group"], c.get("chains", 1))
             result[n] = dict(c, cached=True)
             continue
         tried = []
-        for i1, i2, g in candidates(n, groups):
+        for i1, i2, g, ch in candidates(n, groups, chains):
             try:
-                bank.configure(n, i1, i2, g)
+                bank.configure(n, i1, i2, g, ch)
                 bank.run(templates, so)
                 ms = time_replays(bank, reps, flush)
             except Exception as e:  # a configuration that does not fit this device
-                tried.append({"pass1": i1, "pass2": i2, "group": g, "error": str(e)})
+                tried.append({"pass1": i1, "pass2": i2, "group": g, "chains": ch, "error": str(e)})
                 continue
-            tried.append({"pass1": i1, "pass2": i2, "group": g, "ms": ms})
+            tried.append({"pass1": i1, "pass2": i2, "group": g, "chains": ch, "ms": ms})
         ok = [t for t in tried if "ms" in t]
         if not ok:
-            bank.configure(n, 0, 0, 0)
+            bank.configure(n, 0, 0, 0, 0)
             continue
         best = min(ok, key=lambda t: t["ms"])
-        bank.configure(n, best["pass1"], best["pass2"], best["group"])
+        bank.configure(n, best["pass1"], best["pass2"], best["group"], best["chains"])
         result[n] = dict(best, tried=tried)
-        cache[key] = {k: best[k] for k in ("pass1", "pass2", "group", "ms")}
+        cache[key] = {k: best[k] for k in ("pass1", "pass2", "group", "chains", "ms")}
     if use_cache:
         save_cache(cache, cache_path)
     del flush

@@ -397,6 +397,8 @@ extern "C" int brp_cuda_profile_counters(brp_ctx* c, char* buffer, size_t length
 struct brp_bank {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // second chain of the graph
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::vector<uint32_t> n, unpadded;
     std::vector<float*> d_series;
     std::map<uint32_t, LengthPlan> plans;  // by n
@@ -405,7 +407,8 @@ struct brp_bank {
         float* power = nullptr;
         double* partial = nullptr;
         uint32_t group = 0;                 // templates per launch
-        uint32_t capacity = 0;              // templates the buffers hold
+        uint32_t chains = 1;                // independent launch chains (streams) in the graph
+        uint32_t capacity = 0;              // templates the buffers hold (group * chains)
         uint32_t partial_per_template = 0;  // pass-1 partial sums per template
     };
     std::map<uint32_t, ClassBuffers> classes;
@@ -454,6 +457,9 @@ struct brp_bank {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (done) cudaEventDestroy(done);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
         for (auto p : allocations) cudaFree(p);
         for (auto& kv : plans) free_length_plan(kv.second);
         if (h_params) cudaFreeHost(h_params);
@@ -490,6 +496,10 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return cleanup(st);
     if ((st = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) return cleanup(st);
     if ((st = b->cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "cudaEventCreate"))) return cleanup(st);
+    if ((st = b->cuda(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (st = b->cuda(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate")) ||
+        (st = b->cuda(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming), "cudaEventCreate")))
+        return cleanup(st);
     b->n.assign(n, n + series_count);
     b->unpadded.assign(unpadded, unpadded + series_count);
     b->max_templates = max_templates;
@@ -551,19 +561,24 @@ extern "C" int brp_cuda_bank_set_series(brp_bank* b, uint32_t s, const float* in
 struct KernelEvents { std::vector<int> kind; std::vector<cudaEvent_t> ev; };
 static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, const std::vector<uint32_t>& spans,
                         uint32_t count, KernelEvents* prof = nullptr) {
+    cudaStream_t s = b->stream;
     auto mark = [&](int kind, bool start) {
         if (!prof) return;
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, b->stream);
+        cudaEventRecord(e, s);
         prof->ev.push_back(e);
         if (start) prof->kind.push_back(kind);
     };
-    cudaStream_t s = b->stream;
     cudaMemsetAsync(b->d_counts, 0, count * sizeof(uint32_t), s);
     cudaMemsetAsync(b->d_status, 0, count * sizeof(uint32_t), s);
+    // Groups of a class alternate between the chains (the main stream and the
+    // side stream), each chain with its own intermediate buffers, so that one
+    // group's kernels overlap another's.  Profiling replays use one chain.
+    bool forked = false;
     uint32_t kernels = 0;
     uint32_t t = 0;
+    std::map<uint32_t, uint32_t> groups_done;
     while (t < count) {
         const uint32_t n = sorted_n[t];
         const LengthPlan& lp = b->plans.at(n);
@@ -571,13 +586,24 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         uint32_t end = t;
         while (end < count && sorted_n[end] == n && end - t < cb.group) ++end;
         const uint32_t g = end - t;
+        const uint32_t chain = prof ? 0 : groups_done[n]++ % cb.chains;
+        cudaStream_t cs = s;
+        if (chain == 1) {
+            if (!forked) {
+                cudaEventRecord(b->fork, s);
+                cudaStreamWaitEvent(b->side, b->fork, 0);
+                forked = true;
+            }
+            cs = b->side;
+        }
         FusedArgs a{};
         a.inputs = b->d_inputs + t;
         a.params = b->d_params + t;
         fill_fused_args(a, lp);
-        a.work = cb.work; a.work_stride = lp.M;
-        a.power = cb.power; a.power_stride = lp.M;
-        a.partial = cb.partial; a.partial_stride = lp.blocks1();  // per template, within partial_per_template
+        a.work = cb.work + size_t(chain) * cb.group * lp.M; a.work_stride = lp.M;
+        a.power = cb.power + size_t(chain) * cb.group * lp.M; a.power_stride = lp.M;
+        a.partial = cb.partial + size_t(chain) * cb.group * cb.partial_per_template;
+        a.partial_stride = lp.blocks1();
         a.mean = b->d_mean + t; a.status = b->d_status + t; a.counts = b->d_counts + t;
         a.cands = b->d_cands + size_t(t) * b->capacity;
         a.capacity = b->capacity;
@@ -585,16 +611,20 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         uint32_t span = 0;
         for (uint32_t u = t; u < end; ++u) span = std::max(span, spans[u]);
         mark(0, true);
-        launch_fused_pass1(a, lp, g, s);
+        launch_fused_pass1(a, lp, g, cs);
         mark(0, false);
         mark(1, true);
-        launch_fused_pass2(a, lp, g, s);
+        launch_fused_pass2(a, lp, g, cs);
         mark(1, false);
         mark(2, true);
-        launch_fused_harmonic(a, lp, g, span, s);
+        launch_fused_harmonic(a, lp, g, span, cs);
         mark(2, false);
         kernels += 3;
         t = end;
+    }
+    if (forked) {
+        cudaEventRecord(b->join, b->side);
+        cudaStreamWaitEvent(s, b->join, 0);
     }
     mark(3, true);
     launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_compact, b->compact_cap, b->d_offsets, s);
@@ -692,7 +722,8 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     return BRP_OK;
 }
 
-extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group) {
+extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
+                                       uint32_t chains) {
     if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
     auto it = b->plans.find(n);
     if (it == b->plans.end()) return b->fail(BRP_E_ARGUMENT, "no series of that length");
@@ -705,10 +736,11 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
     if (!lp.fused) { free_length_plan(lp); return b->fail(BRP_E_ARGUMENT, "no fused plan for that configuration"); }
     brp_bank::ClassBuffers& cb = b->classes.at(n);
     const uint32_t g = group ? std::min(group, b->max_templates) : cb.group;
-    if (g > cb.capacity || lp.blocks1() > cb.partial_per_template) {
+    const uint32_t ch = chains ? std::min(chains, 2u) : cb.chains;
+    if (g * ch > cb.capacity || lp.blocks1() > cb.partial_per_template) {
         // grow the class buffers
         brp_bank::ClassBuffers nb;
-        nb.capacity = std::max(g, cb.capacity);
+        nb.capacity = std::max(g * ch, cb.capacity);
         nb.partial_per_template = std::max(lp.blocks1(), cb.partial_per_template);
         if ((st = b->alloc(&nb.work, size_t(nb.capacity) * lp.M, "work")) ||
             (st = b->alloc(&nb.power, size_t(nb.capacity) * lp.M, "power")) ||
@@ -720,6 +752,7 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
         cb.capacity = nb.capacity; cb.partial_per_template = nb.partial_per_template;
     }
     cb.group = g;
+    cb.chains = ch;
     free_length_plan(it->second);
     it->second = lp;
     b->graph_key.clear();

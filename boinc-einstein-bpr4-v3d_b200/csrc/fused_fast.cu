@@ -168,19 +168,37 @@ __device__ __forceinline__ double gather(float* smf, const float* __restrict__ i
     float* dst = smf + 2 * ((rem >> 1) * STRIDE + smem_pos(n1_0)) + (rem & 1);
     constexpr int DSTEP = 2 * (ROWS_STEP + ROWS_STEP / 16);
     float sum = 0.f;
-#pragma unroll 4
-    for (int q = 0; q < PER; ++q, i += istep, dst += DSTEP) {
-        float v = 0.f;
-        if (i < steps) {
-            int j;
-            if (MODE == 2) j = brp_resample_index_fp64(i, rc);
-            else j = lean_index<MODE == 1>(i, rc);
-            if (uint32_t(j) < unpadded) v = __ldg(in + j);
-            else oob = true;
-            if (raw) raw[i] = v;
+    // Indices for a batch of samples first, then all of the batch's loads, so
+    // each thread keeps BATCH gathers in flight.
+    constexpr int BATCH = 8;
+    static_assert(PER % BATCH == 0, "batch must divide the samples per thread");
+#pragma unroll 1
+    for (int q0 = 0; q0 < PER; q0 += BATCH) {
+        int j[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b) {
+            const uint32_t ib = i + uint32_t(b) * istep;
+            j[b] = -1;
+            if (ib < steps) {
+                int jj;
+                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
+                else jj = lean_index<MODE == 1>(ib, rc);
+                if (uint32_t(jj) < unpadded) j[b] = jj;
+                else oob = true;
+            }
         }
-        sum += v;
-        *dst = v;
+        float v[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b) v[b] = j[b] >= 0 ? __ldg(in + j[b]) : 0.f;
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b) {
+            const uint32_t ib = i + uint32_t(b) * istep;
+            if (raw && ib < steps) raw[ib] = v[b];
+            sum += v[b];
+            dst[b * DSTEP] = v[b];
+        }
+        i += BATCH * istep;
+        dst += BATCH * DSTEP;
     }
     return double(sum);
 }

@@ -201,3 +201,23 @@ extern "C" uint32_t brp_toplist_final(const brp_toplist* t, brp_bank_candidate* 
     }
     return count;
 }
+
+// The bank loop of src/workunit_main.cpp:77-124 after the search: for each
+// template in bank order, raise its thresholds to the toplist's current row
+// 100 (Toplist::thresholds) and retain its candidates (Toplist::retain).
+// candidates holds the templates' lists back to back; counts[t] per template;
+// orbits[t] = (period, tau, psi).
+extern "C" int brp_toplist_fold(brp_toplist* t, const brp_params* templates, const double* orbits,
+                                const brp_candidate* candidates, const uint32_t* counts, uint32_t count) {
+    if (!t || !templates || !orbits || !counts || (!candidates && count)) return host_fail("null argument");
+    uint64_t off = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        brp_params p = templates[k];
+        brp_toplist_thresholds(t, &p);
+        const int st = brp_toplist_retain(t, candidates + off, counts[k], orbits[3 * k], orbits[3 * k + 1],
+                                          orbits[3 * k + 2], &p);
+        if (st) return st;
+        off += counts[k];
+    }
+    return BRP_OK;
+}

@@ -136,9 +136,11 @@ int brp_cuda_bank_set_series(brp_bank* bank, uint32_t series, const float* input
 int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count,
                       brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status);
 /* Selects the kernels of one length class: compiled pass-1 / pass-2
- * configuration ids (0 = default, -1 = generic kernels) and templates per
- * launch (0 = keep).  Used by the autotuner; the next run re-captures. */
-int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group);
+ * configuration ids (0 = default, -1 = generic kernels), templates per
+ * launch and independent launch chains in the graph (1 or 2; 0 = keep).
+ * Used by the autotuner; the next run re-captures. */
+int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
+                            uint32_t chains);
 /* Lists the compiled configurations: ids, sequence length L (pass 1: column
  * length L1, pass 2: row length L2) and kind (1 = pass 1, 2 = pass 2).
  * Returns the total count; writes at most cap entries. */
@@ -182,6 +184,13 @@ int brp_toplist_retain(brp_toplist* t, const brp_candidate* candidates, uint32_t
                        double psi, const brp_params* p);
 /* Writes up to 100 final candidates; returns how many. */
 uint32_t brp_toplist_final(const brp_toplist* t, brp_bank_candidate* out);
+/* The bank loop after the search (src/workunit_main.cpp:77-124): for each of
+ * count templates in bank order, raise its thresholds to the toplist's current
+ * rows (thresholds) and retain its candidates (retain).  candidates: the
+ * templates' lists back to back, counts[t] each; orbits: 3 doubles (period,
+ * tau, psi) per template. */
+int brp_toplist_fold(brp_toplist* t, const brp_params* templates, const double* orbits,
+                     const brp_candidate* candidates, const uint32_t* counts, uint32_t count);
 
 #ifdef __cplusplus
 }

@@ -108,3 +108,21 @@ def test_toplist_rejects_invalid_candidate():
     c["bin"], c["level"], c["power"] = p.fundamental, 0, 100.0
     with pytest.raises(B.BrpError):
         t.retain(c, 1.0, 0.0, 0.0, p)
+
+
+def test_toplist_fold_equals_sequential_retain(oracle):
+    rng = np.random.default_rng(12)
+    p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
+    temps, orbs, cands = [], [], []
+    for t in range(200):
+        q = p.copy()
+        for h in range(5):
+            q.threshold[h] = p.threshold[h] * float(rng.uniform(0.95, 1.05))
+        temps.append(q)
+        orbs.append((3600.0 + t, 0.01 * t, 0.1 * t))
+        cands.append(_random_candidates(rng, q, int(rng.integers(0, 25))))
+    a = B.Toplist().fold(temps, orbs, cands).final()
+    ref = oracle.Toplist()
+    for q, o, c in zip(temps, orbs, cands):
+        ref.retain(c, *o, ref.thresholds(q))
+    assert a.tobytes() == ref.final().tobytes() and len(a) > 0
