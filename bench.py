@@ -246,10 +246,13 @@ def main():
     stream = torch.cuda.ExternalStream(bank.stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
+    tarr = B.Bank.params_array(my_templates)
+    orbits = np.asarray(wl.orbits[begin:end], np.float64)
+    outbuf = np.empty(count * CAPACITY, B.CANDIDATE)
+
     def e2e_step():
         bank.set_series(0, x_host)
-        cands, counts, status = bank.run(my_templates)
-        return cands
+        return bank.run_flat(tarr, out=outbuf)
 
     # autotune the kernel configuration and templates per launch on this bank
     # (untimed), then warm up through the public API (captures the graph)
@@ -262,8 +265,8 @@ def main():
         if os.environ.get("BRP_BENCH_VERBOSE"):
             print(json.dumps({"tuning": {str(n): r.get("tried") for n, r in res.items()}}), file=sys.stderr)
     for _ in range(max(args.warmup, 3)):
-        cands = e2e_step()
-    d2h = 4 * count * 2 + 8 * (count + 1) + 16 * sum(len(c) for c in cands)
+        flat, offs, counts, status = e2e_step()
+    d2h = 4 * count * 2 + 8 * (count + 1) + 16 * len(flat)
     h2d = 4 * N + 108 * count + 8 * count
 
     def barrier():
@@ -294,9 +297,9 @@ def main():
     t0 = time.perf_counter()
     top = B.Toplist()
     for _ in range(args.steps):
-        cands = e2e_step()
+        flat, offs, counts, status = e2e_step()
         if world == 1:
-            shard.fold_toplist(top, my_templates, wl.orbits[begin:end], cands)
+            top.fold(tarr, orbits, flat, counts)
     torch.cuda.synchronize()
     e2e_ms = 1000 * (time.perf_counter() - t0)
     barrier()

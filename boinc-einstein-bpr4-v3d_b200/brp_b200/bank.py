@@ -40,30 +40,41 @@ class Bank:
             raise BrpError(4, "series length mismatch")
         check(lib().brp_cuda_bank_set_series(self._b, index, ptr(x)), self._err)
 
+    @staticmethod
+    def params_array(templates):
+        """A ctypes array of the templates (reusable across runs)."""
+        return (Params * len(templates))(*[as_params(t) for t in templates])
+
     def run(self, templates, series_of=None, out=None):
         """Searches every template; returns (candidates per template, counts, status).
         Raises BrpError when a template overflowed or resampled out of range."""
-        count = len(templates)
-        arr = (Params * count)(*[as_params(t) for t in templates])
+        flat, offs, counts, status = self.run_flat(templates, series_of, out)
+        return [flat[offs[t]:offs[t + 1]] for t in range(len(counts))], counts, status
+
+    def run_flat(self, templates, series_of=None, out=None):
+        """As run(), returning the candidates back to back: (candidates,
+        offsets[count + 1], counts, status).  `templates` may be a list of
+        Params or an array from params_array()."""
+        arr = templates if isinstance(templates, ctypes.Array) else self.params_array(templates)
+        count = len(arr)
         so = np.zeros(count, np.uint32) if series_of is None else np.ascontiguousarray(series_of, dtype=np.uint32)
         counts = np.zeros(count, np.uint32)
         status = np.zeros(count, np.uint32)
         cap = count * self.capacity
         if out is None:
-            if self._out.size < cap:
-                self._out = np.empty(cap, CANDIDATE)
-            out = self._out
+            out = np.empty(cap, CANDIDATE)
         st = lib().brp_cuda_bank_run(self._b, arr, ptr(so), count, ptr(out), out.size, ptr(counts), ptr(status))
         if st and st != 2:
             check(st, self._err)
         offs = np.zeros(count + 1, np.int64)
         offs[1:] = np.cumsum(np.minimum(counts, self.capacity).astype(np.int64))
-        result = [out[offs[t]:offs[t + 1]].copy() for t in range(count)]
+        flat = out[:offs[-1]]
         if st:
             e = BrpError(st, self._err())
-            e.counts, e.status, e.candidates = counts, status, result
+            e.counts, e.status = counts, status
+            e.candidates = [flat[offs[t]:offs[t + 1]] for t in range(count)]
             raise e
-        return result, counts, status
+        return flat, offs, counts, status
 
     def configure(self, n, pass1=0, pass2=0, group=0, chains=0):
         """Selects compiled pass configurations, templates per launch and

@@ -72,13 +72,21 @@ class Toplist:
         if st:
             raise BrpError(st, "invalid compact candidate")
 
-    def fold(self, templates, orbits, candidates):
-        """Thresholds + retain for every template in bank order, in one call."""
-        count = len(templates)
-        arr = (Params * count)(*[as_params(t) for t in templates])
+    def fold(self, templates, orbits, candidates, counts=None):
+        """Thresholds + retain for every template in bank order, in one call.
+        `candidates` is a list of per-template arrays, or (with `counts`) the
+        flat array of Bank.run_flat; `templates` a list or a Params array."""
+        arr = templates if isinstance(templates, ctypes.Array) else \
+            (Params * len(templates))(*[as_params(t) for t in templates])
+        count = len(arr)
         orb = np.ascontiguousarray(orbits, dtype=np.float64).reshape(count, 3)
-        counts = np.array([len(c) for c in candidates], np.uint32)
-        flat = np.ascontiguousarray(np.concatenate(candidates) if count else np.zeros(0, CANDIDATE), dtype=CANDIDATE)
+        if counts is None:
+            counts = np.array([len(c) for c in candidates], np.uint32)
+            flat = np.ascontiguousarray(np.concatenate(candidates) if count else np.zeros(0, CANDIDATE),
+                                        dtype=CANDIDATE)
+        else:
+            counts = np.ascontiguousarray(counts, dtype=np.uint32)
+            flat = np.ascontiguousarray(candidates, dtype=CANDIDATE)
         st = lib().brp_toplist_fold(self._t, arr, ptr(orb), ptr(flat), ptr(counts), count)
         if st:
             raise BrpError(st, "invalid compact candidate")

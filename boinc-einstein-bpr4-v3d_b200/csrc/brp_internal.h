@@ -36,6 +36,7 @@ struct LengthPlan {
     const FastPass* fp1 = nullptr;  // compiled pass 1 / pass 2 (nullptr: generic kernels)
     const FastPass* fp2 = nullptr;
     const float2 *ptw1 = nullptr, *ptw2 = nullptr;
+    const float2 *hf_hi = nullptr, *hf_lo = nullptr;  // W_{2n}^e (cos, -sin of pi e / n)
     float2* d_tables = nullptr;
     size_t tables_bytes = 0;
     const float2 *tw1 = nullptr, *tw2 = nullptr, *fs_hi = nullptr, *fs_lo = nullptr, *rl_hi = nullptr,
@@ -49,6 +50,13 @@ struct LengthPlan {
 // error message or empty.  fast1/fast2 (optional) force compiled pass
 // configurations by id (0: default choice, -1: generic kernels).
 std::string make_length_plan(uint32_t n, LengthPlan& plan, cudaStream_t stream, int fast1 = 0, int fast2 = 0);
+// The parts of make_length_plan: the decomposition and kernel choice (no
+// allocation), the table layout (offsets[12], returns the float2 count;
+// with_plain adds the table of the step-by-step pipeline) and the table fill
+// (host[] laid out by the layout, lp's views pointed at dev).
+std::string choose_length_plan(uint32_t n, LengthPlan& plan, int fast1 = 0, int fast2 = 0);
+size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t offsets[12]);
+void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, float2* dev);
 void free_length_plan(LengthPlan& plan);
 
 constexpr uint32_t kSplitLog2 = 11;
@@ -80,6 +88,7 @@ struct FusedArgs {
     int plan1[7], plan2[7];      // count followed by radices
     const float2 *tw1, *tw2, *fs_hi, *fs_lo, *rl_hi, *rl_lo;
     const float2 *ptw1, *ptw2;  // per-pass twiddle tables of the compiled passes
+    const float2 *hf_hi, *hf_lo;  // W_{2n}^e: (cos(pi e/n), -sin(pi e/n)), e <= M
     float2* work;     // per template: M complex (four-step intermediate)
     size_t work_stride;
     float* power;     // per template: M floats (P[k] = |X_k|^2 / n, P[0] = 0)

@@ -313,12 +313,13 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
                     if (fft) fft[M] = make_float2(zk.x - zk.y - (a_odd ? mean : 0.f), 0.f);
                     Pw[0] = 0.f;
                 } else {
-                    float sv, cv;
-                    sincospif(float(k) / fn, &sv, &cv);
+                    const float2 hf = twiddle2(a.hf_hi, a.hf_lo, kSplitLog2, k);
+                    const float cv = hf.x, sv = -hf.y;
+                    const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
                     const float2 wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
                     const float2 G = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
                     const float f = __fdividef(-0.5f * mean, sv);
-                    X = real_bin(zk, zm, twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, k), make_float2(G.x * f, G.y * f));
+                    X = real_bin(zk, zm, w, make_float2(G.x * f, G.y * f));
                     const float pw = X.x * X.x + X.y * X.y;
                     Pw[k] = pow2 ? pw * inv_n : pw / fn;
                 }

@@ -66,7 +66,7 @@ static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
     }
 }
 
-std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream, int fast1, int fast2) {
+std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2) {
     const bool radix3 = !is_pow2(n);
     if (n < 64 || n > 3u * (1u << 22) || (radix3 && !(n % 3 == 0 && is_pow2(n / 3))))
         return "series length must be 2^k or 3*2^k in 64..3*2^22";
@@ -118,39 +118,70 @@ std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream, in
     }
     if (lp.fused && set_harmonic_fast_attributes() != cudaSuccess)
         return "cannot enable the shared memory of the harmonic kernel";
-    // Tables: tw1[L1] tw2[L2] fs_hi[ceil(M/2048)] fs_lo[2048] rl_hi[ceil(n/2048)] rl_lo[2048] twb[B]
-    // ptw1 ptw2 (per-pass tables of the compiled passes); each block 16-byte aligned.
-    const uint32_t split = 1u << kSplitLog2;
+    return "";
+}
+
+// Table layout of a chosen plan: offsets (float2 entries) of tw1, tw2, fs_hi,
+// fs_lo, rl_hi, rl_lo, twb, ptw1, ptw2, hf_hi, hf_lo and the total.  Tables:
+// tw1[L1] tw2[L2] fs_hi[ceil(M/2048)] fs_lo[2048] rl_hi[ceil(n/2048)] rl_lo[2048]
+// twb[B] (only with_plain) ptw1 ptw2 (per-pass tables of the compiled passes)
+// hf_hi[ceil((M+1)/2048)] hf_lo[2048] (W_{2n}^e = cos(pi e/n) - i sin(pi e/n),
+// e <= M); each block 16-byte aligned.
+size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t off[12]) {
+    const uint32_t split = 1u << kSplitLog2, n = lp.n;
     const uint32_t fs_hi_n = (lp.M + split - 1) / split, rl_hi_n = (n + split - 1) / split;
-    std::vector<size_t> off(10, 0);
+    const uint32_t hf_hi_n = (lp.M + 1 + split - 1) / split;
+    const uint32_t counts[11] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, with_plain ? lp.B : 0u,
+                                 uint32_t(lp.fp1 ? lp.fp1->table : 0), uint32_t(lp.fp2 ? lp.fp2->table : 0),
+                                 hf_hi_n, split};
     size_t total = 0;
-    const uint32_t counts[9] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, lp.B,
-                                uint32_t(lp.fp1 ? lp.fp1->table : 0), uint32_t(lp.fp2 ? lp.fp2->table : 0)};
-    for (int i = 0; i < 9; ++i) { off[i] = total; total += (counts[i] + 1) & ~1u; }
-    std::vector<float2> host(total);
-    if (lp.L1) fill_twiddles(host.data() + off[0], lp.L1, lp.L1, 0, 1);
-    if (lp.L2) fill_twiddles(host.data() + off[1], lp.L2, lp.L2, 0, 1);
-    fill_twiddles(host.data() + off[2], fs_hi_n, lp.M, 0, split);
-    fill_twiddles(host.data() + off[3], split, lp.M, 0, 1);
-    fill_twiddles(host.data() + off[4], rl_hi_n, n, 0, split);
-    fill_twiddles(host.data() + off[5], split, n, 0, 1);
-    fill_twiddles(host.data() + off[6], lp.B, lp.B, 0, 1);
-    if (lp.fp1) fill_pass_tables(host.data() + off[7], lp.plan1);
-    if (lp.fp2) fill_pass_tables(host.data() + off[8], lp.plan2);
+    for (int i = 0; i < 11; ++i) { off[i] = total; total += (counts[i] + 1) & ~1u; }
+    off[11] = total;
+    return total;
+}
+
+// Fills the tables of lp into host[] (laid out by length_plan_layout) and
+// points lp's table views at dev (the device copy of host[]).
+void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, float2* dev) {
+    size_t off[12];
+    length_plan_layout(lp, with_plain, off);
+    const uint32_t split = 1u << kSplitLog2, n = lp.n;
+    if (lp.L1) fill_twiddles(host + off[0], lp.L1, lp.L1, 0, 1);
+    if (lp.L2) fill_twiddles(host + off[1], lp.L2, lp.L2, 0, 1);
+    fill_twiddles(host + off[2], uint32_t(off[3] - off[2]) & ~0u, lp.M, 0, split);
+    fill_twiddles(host + off[3], split, lp.M, 0, 1);
+    fill_twiddles(host + off[4], uint32_t(off[5] - off[4]), n, 0, split);
+    fill_twiddles(host + off[5], split, n, 0, 1);
+    if (with_plain) fill_twiddles(host + off[6], lp.B, lp.B, 0, 1);
+    if (lp.fp1) fill_pass_tables(host + off[7], lp.plan1);
+    if (lp.fp2) fill_pass_tables(host + off[8], lp.plan2);
+    fill_twiddles(host + off[9], uint32_t(off[10] - off[9]), 2ull * n, 0, split);
+    fill_twiddles(host + off[10], split, 2ull * n, 0, 1);
+    lp.tw1 = dev + off[0];
+    lp.tw2 = dev + off[1];
+    lp.fs_hi = dev + off[2];
+    lp.fs_lo = dev + off[3];
+    lp.rl_hi = dev + off[4];
+    lp.rl_lo = dev + off[5];
+    lp.twb = with_plain ? dev + off[6] : nullptr;
+    lp.ptw1 = dev + off[7];
+    lp.ptw2 = dev + off[8];
+    lp.hf_hi = dev + off[9];
+    lp.hf_lo = dev + off[10];
+}
+
+std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream, int fast1, int fast2) {
+    std::string e = choose_length_plan(n, lp, fast1, fast2);
+    if (!e.empty()) return e;
+    size_t off[12];
+    const size_t total = length_plan_layout(lp, true, off);
     lp.tables_bytes = total * sizeof(float2);
     if (cudaMalloc(&lp.d_tables, lp.tables_bytes) != cudaSuccess) return "cudaMalloc of twiddle tables failed";
+    std::vector<float2> host(total);
+    fill_length_plan_tables(lp, true, host.data(), lp.d_tables);
     if (cudaMemcpyAsync(lp.d_tables, host.data(), lp.tables_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
         return "upload of twiddle tables failed";
-    lp.tw1 = lp.d_tables + off[0];
-    lp.tw2 = lp.d_tables + off[1];
-    lp.fs_hi = lp.d_tables + off[2];
-    lp.fs_lo = lp.d_tables + off[3];
-    lp.rl_hi = lp.d_tables + off[4];
-    lp.rl_lo = lp.d_tables + off[5];
-    lp.twb = lp.d_tables + off[6];
-    lp.ptw1 = lp.d_tables + off[7];
-    lp.ptw2 = lp.d_tables + off[8];
     return "";
 }
 
