@@ -81,7 +81,7 @@ EXPORTS = (
     "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_configure", "brp_cuda_fast_configs", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
     "brp_cuda_bank_last_error", "brp_host_parameters", "brp_host_resampling_steps", "brp_host_search_parameters",
     "brp_toplist_create", "brp_toplist_destroy", "brp_toplist_thresholds", "brp_toplist_retain",
-    "brp_toplist_final", "brp_toplist_fold",
+    "brp_toplist_final", "brp_toplist_fold", "brp_cuda_search_static", "brp_cuda_search_static_error",
 )
 
 
@@ -117,6 +117,8 @@ def lib():
             L.brp_cuda_bank_destroy.restype = None
             L.brp_cuda_bank_set_series.argtypes = [vp, u32, vp]
             L.brp_cuda_bank_run.argtypes = [vp, vp, vp, u32, vp, u64, vp, vp]
+            L.brp_cuda_search_static.argtypes = [P, vp, vp, vp, u32, vp, vp, vp]
+            L.brp_cuda_search_static_error.restype = ctypes.c_char_p
             L.brp_cuda_bank_launch.argtypes = [vp]
             L.brp_cuda_bank_configure.argtypes = [vp, u32, ctypes.c_int32, ctypes.c_int32, u32, u32]
             L.brp_cuda_fast_configs.argtypes = [vp, vp, vp, u32]

@@ -160,6 +160,33 @@ int brp_cuda_bank_profile(brp_bank* bank, double* kernel_ms, uint32_t* launches)
 uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* bank);
 const char* brp_cuda_bank_last_error(const brp_bank* bank);
 
+/* ---- Search without device allocation ----
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory while they run (a plugin limited to the buffers its host hands it, a
+ * process whose device memory belongs to another framework's pool, a
+ * real-time loop that must not block in the allocator): one template through
+ * the fused search (resampling, packed real FFT, power spectrum, harmonic
+ * summing, candidate compaction) with all working memory in a static device
+ * array inside this library (about 4.2 MiB, held by every GPU that loads the
+ * library until the process exits).  It calls no cudaMalloc or cudaFree.
+ *   input      device, params->unpadded floats (the series)
+ *   power      device, n/2 floats (P[k] = |X_k|^2 / n, P[0] = 0)
+ *   candidates device, capacity entries; *count (device) the number found,
+ *              which may exceed capacity; *status (device) BRP_STATUS_* bits
+ *   stream     cudaStream_t (NULL: legacy default stream)
+ * Series lengths 8192..1048576 (2^k or 3*2^k); longer ones are rejected with
+ * BRP_E_ARGUMENT.  The call is asynchronous on `stream`; results are valid
+ * once the stream has completed.  The first call on a device (and the first
+ * call with a new series length) does set-up -- the scratch array's device
+ * address, kernel attributes, the twiddle tables copied into the array --
+ * so it must come before any stream capture.  Every call shares the one
+ * array, which keeps the last call's contents: calls that overlap on the GPU
+ * (other streams, other threads) race and must be serialised by the caller.
+ * brp_cuda_search_static_error() gives the calling thread's last message. */
+int brp_cuda_search_static(const brp_params* params, const float* input, float* power, brp_candidate* candidates,
+                           uint32_t capacity, uint32_t* count, uint32_t* status, void* stream);
+const char* brp_cuda_search_static_error(void);
+
 /* ---- Host helpers (the reference's host code around the path) ---- */
 /* src/science.cpp:46-65 (brp::parameters). */
 int brp_host_parameters(uint32_t n, uint32_t unpadded, float tau, float period, float psi, float dt,
