@@ -312,6 +312,12 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_ms, e2e_ms = t.tolist()
 
+    # the spectrum error of this build on the bench workload: one template's
+    # power against an FP64 FFT of the same padded series
+    accuracy = None
+    if rank == 0:
+        accuracy = spectrum_error(B, wl, my_templates[0])
+
     # plain per-template pipeline on the same GPU (comparator)
     plain = None
     if rank == 0 and not args.no_plain:
@@ -360,6 +366,8 @@ def main():
         "algorithmic_gbs_all_kernels": 16 * N * count / (sum(kernel_ms[k] for k in ALGO_BYTES) * 1e-3) / 1e9,
         "clocks": clock,
     }
+    if accuracy:
+        line["accuracy"] = accuracy
     if plain:
         line["plain"] = plain
         line["batched_vs_plain"] = value / world / plain["templates_per_s"]
@@ -368,6 +376,21 @@ def main():
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def spectrum_error(B, wl, p):
+    """Relative RMS of the GPU power spectrum against numpy's FP64 real FFT of
+    the GPU's own padded series (isolates the FFT and power arithmetic)."""
+    g = B.GPU(p, wl.series[0], 256, 0, 1, stockham=True, packed=True)
+    g.set_template(p)
+    g.run()
+    s = g.snapshot()
+    g.close()
+    X = np.fft.rfft(s.resampled.astype(np.float64))
+    P = (X.real[: p.n // 2] ** 2 + X.imag[: p.n // 2] ** 2) / p.n
+    P[0] = 0
+    err = float(np.sqrt(np.sum((s.power - P) ** 2) / np.sum(P ** 2)))
+    return {"power_rel_rms_vs_fp64": err, "template": "bank template 0", "bar": 2e-6}
 
 
 def time_plain(B, wl, templates):
