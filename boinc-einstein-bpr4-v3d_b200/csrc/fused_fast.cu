@@ -27,6 +27,11 @@ __constant__ uint32_t c_fast_lut_bits[130] = BRP_LUT_BITS;
 
 namespace {
 
+// Shared-memory layout of the compiled kernels: element e of a sequence at
+// e + e / 16 (one padding slot per 16 keeps radix-16 strided stores on distinct
+// banks).  Sequences sit `stride` elements apart, stride = 16/G (mod 16)
+// (G = sequences a warp touches side by side).
+__host__ __device__ constexpr int ct_pos(int e) { return e + (e >> 4); }
 __host__ __device__ constexpr int ct_stride(int L, int G) {
     int base = L + L / 16;
     int want = (G >= 16) ? 1 : 16 / G;
@@ -36,10 +41,25 @@ __host__ __device__ constexpr int ct_stride(int L, int G) {
 
 template <int R> struct TwStride { static constexpr int value = (R + 1) & ~1; };
 
+template <int R, int Ns>
+__device__ __forceinline__ void ct_twiddle(float2* v, const float2* __restrict__ tw, int k) {
+    if constexpr (Ns > 1) {
+        constexpr int RS = TwStride<R>::value;
+        const float4* w4 = reinterpret_cast<const float4*>(tw + k * RS);
+#pragma unroll
+        for (int r = 1; r < R; r += 2) {
+            const float4 w = __ldg(w4 + (r - 1) / 2);
+            v[r] = cmul(v[r], make_float2(w.x, w.y));
+            if (r + 1 < R) v[r + 1] = cmul(v[r + 1], make_float2(w.z, w.w));
+        }
+    }
+}
+
+// One Stockham pass: each thread loads its butterflies' inputs, the CTA
+// synchronises, then each thread twiddles, transforms and stores in place.
 template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
 __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ tw) {
     constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
-    constexpr int RS = TwStride<R>::value;
     float2 v[PER][R];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
@@ -48,7 +68,7 @@ __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ 
             const int c = b / NBF, j = b - c * NBF;
             const float2* src = buf + c * STRIDE;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = src[smem_pos(j + r * NBF)];
+            for (int r = 0; r < R; ++r) v[q][r] = src[ct_pos(j + r * NBF)];
         }
     }
     __syncthreads();
@@ -58,20 +78,12 @@ __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ 
         if (TOTAL % THREADS == 0 || b < TOTAL) {
             const int c = b / NBF, j = b - c * NBF;
             const int k = j % Ns;
-            if constexpr (Ns > 1) {
-                const float4* w4 = reinterpret_cast<const float4*>(tw + k * RS);
-#pragma unroll
-                for (int r = 1; r < R; r += 2) {
-                    const float4 w = __ldg(w4 + (r - 1) / 2);
-                    v[q][r] = cmul(v[q][r], make_float2(w.x, w.y));
-                    if (r + 1 < R) v[q][r + 1] = cmul(v[q][r + 1], make_float2(w.z, w.w));
-                }
-            }
+            ct_twiddle<R, Ns>(v[q], tw, k);
             dft<R>(v[q]);
             float2* dst = buf + c * STRIDE;
             const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[smem_pos(base + r * Ns)] = v[q][r];
+            for (int r = 0; r < R; ++r) dst[ct_pos(base + r * Ns)] = v[q][r];
         }
     }
     __syncthreads();
@@ -149,35 +161,36 @@ __device__ __forceinline__ double block_sum_d(double v, double* scratch) {
     return r;
 }
 
-// Gathers this CTA's samples (rows n1 < L1, 2C consecutive reals per row) into
-// shared memory; returns the sum of the samples (FP32 per thread, at most a few
-// dozen samples, then FP64 across threads).  Thread t always handles the same
-// position rem = t % 2C of its rows, so the sample index, its float value and
-// the shared-memory address advance by constants.
+// Gathers this CTA's samples (rows n1 < L1, C complex points = 2C consecutive
+// reals per row) into shared memory; returns the sum of the samples (FP32 per
+// thread, a few dozen samples, then FP64 across threads).  Thread t handles
+// column t % C of rows t / C + q THREADS / C: the two samples of a complex
+// point, one 64-bit store; sample index and shared address advance by
+// constants.
 template <int L1, int C, int THREADS, int STRIDE, int MODE>
-__device__ __forceinline__ double gather(float* smf, const float* __restrict__ in, const brp_params& P,
+__device__ __forceinline__ double gather(float2* sm, const float* __restrict__ in, const brp_params& P,
                                          uint32_t L2, uint32_t c0, float* raw, bool& oob) {
-    constexpr int ROW = 2 * C, TOTAL = L1 * ROW, PER = TOTAL / THREADS, ROWS_STEP = THREADS / ROW;
-    static_assert(TOTAL % THREADS == 0 && THREADS % ROW == 0, "gather must tile the CTA");
+    constexpr int TOTAL = L1 * C, PER = TOTAL / THREADS, ROWS_STEP = THREADS / C;
+    static_assert(TOTAL % THREADS == 0 && THREADS % C == 0, "gather must tile the CTA");
     static_assert(ROWS_STEP % 16 == 0, "row step must keep the shared-memory padding periodic");
     const brp_resample_consts rc = consts_of(P);
     const uint32_t steps = P.steps, unpadded = P.unpadded;
-    const int rem = threadIdx.x % ROW, n1_0 = threadIdx.x / ROW;
+    const int c = threadIdx.x % C, n1_0 = threadIdx.x / C;
     const uint32_t istep = 2u * L2 * ROWS_STEP;
-    uint32_t i = 2u * (L2 * uint32_t(n1_0) + c0) + uint32_t(rem);
-    float* dst = smf + 2 * ((rem >> 1) * STRIDE + smem_pos(n1_0)) + (rem & 1);
-    constexpr int DSTEP = 2 * (ROWS_STEP + ROWS_STEP / 16);
+    uint32_t i = 2u * (L2 * uint32_t(n1_0) + c0 + uint32_t(c));
+    float2* dst = sm + c * STRIDE + ct_pos(n1_0);
+    constexpr int DSTEP = ROWS_STEP + (ROWS_STEP / 16);
     float sum = 0.f;
-    // Indices for a batch of samples first, then all of the batch's loads, so
-    // each thread keeps BATCH gathers in flight.
-    constexpr int BATCH = 8;
-    static_assert(PER % BATCH == 0, "batch must divide the samples per thread");
+    // Indices of a batch of points first, then all of the batch's loads, so each
+    // thread keeps 2 BATCH gathers in flight.
+    constexpr int BATCH = 4;
+    static_assert(PER % BATCH == 0, "batch must divide the points per thread");
 #pragma unroll 1
     for (int q0 = 0; q0 < PER; q0 += BATCH) {
-        int j[BATCH];
+        int j[2 * BATCH];
 #pragma unroll
-        for (int b = 0; b < BATCH; ++b) {
-            const uint32_t ib = i + uint32_t(b) * istep;
+        for (int b = 0; b < 2 * BATCH; ++b) {
+            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
             j[b] = -1;
             if (ib < steps) {
                 int jj;
@@ -187,15 +200,19 @@ __device__ __forceinline__ double gather(float* smf, const float* __restrict__ i
                 else oob = true;
             }
         }
-        float v[BATCH];
+        float v[2 * BATCH];
 #pragma unroll
-        for (int b = 0; b < BATCH; ++b) v[b] = j[b] >= 0 ? __ldg(in + j[b]) : 0.f;
+        for (int b = 0; b < 2 * BATCH; ++b) v[b] = j[b] >= 0 ? __ldg(in + j[b]) : 0.f;
 #pragma unroll
         for (int b = 0; b < BATCH; ++b) {
-            const uint32_t ib = i + uint32_t(b) * istep;
-            if (raw && ib < steps) raw[ib] = v[b];
-            sum += v[b];
-            dst[b * DSTEP] = v[b];
+            if (raw) {
+                const uint32_t ib = i + uint32_t(b) * istep;
+                if (ib < steps) raw[ib] = v[2 * b];
+                if (ib + 1 < steps) raw[ib + 1] = v[2 * b + 1];
+            }
+            sum += v[2 * b];
+            sum += v[2 * b + 1];
+            dst[b * DSTEP] = make_float2(v[2 * b], v[2 * b + 1]);
         }
         i += BATCH * istep;
         dst += BATCH * DSTEP;
@@ -206,19 +223,18 @@ __device__ __forceinline__ double gather(float* smf, const float* __restrict__ i
 template <int L1, int C, int THREADS, int MINB, int... Rs>
 __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     constexpr int STRIDE = ct_stride(L1, C);
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[THREADS / 32];
     const int g = blockIdx.y;
     const brp_params& P = a.params[g];
     const float* __restrict__ in = a.inputs[g];
     const uint32_t L2 = a.L2, c0 = blockIdx.x * C;
     float* raw = (g == a.snap) ? a.snap_raw : nullptr;
-    float* smf = reinterpret_cast<float*>(sm);
     bool oob = false;
     double sum;
-    if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(smf, in, P, L2, c0, raw, oob);
-    else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(smf, in, P, L2, c0, raw, oob);
-    else sum = gather<L1, C, THREADS, STRIDE, 0>(smf, in, P, L2, c0, raw, oob);
+    if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
+    else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
+    else sum = gather<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
     if (oob) atomicOr(a.status + g, BRP_STATUS_RESAMPLE_OOB);
     const double tot = block_sum_d<THREADS>(sum, red);
     if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
@@ -230,7 +246,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
 #pragma unroll 4
     for (int idx = threadIdx.x; idx < L1 * C; idx += THREADS) {
         const int k1 = idx / C, c = idx % C;
-        float2 y = sm[c * STRIDE + smem_pos(k1)];
+        float2 y = sm[c * STRIDE + ct_pos(k1)];
         const uint32_t e = (c0 + uint32_t(c)) * uint32_t(k1);
         y = cmul(y, twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, e));
         T[size_t(k1) * L2 + c0 + c] = y;
@@ -253,7 +269,7 @@ __device__ __forceinline__ float2 real_bin(float2 zk, float2 zm, float2 w, float
 template <int L2, int R, int THREADS, int MINB, int... Rs>
 __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     constexpr int SEQ = 2 * R, STRIDE = ct_stride(L2, R);
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[THREADS / 32];
     __shared__ float s_mean;
     const int g = blockIdx.y, q = blockIdx.x;
@@ -272,8 +288,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             row = ar == 0 ? L1 / 2 : L1 - ar;
         }
         const float4 x = __ldg(reinterpret_cast<const float4*>(T + size_t(row) * L2 + k2));
-        sm[rr * STRIDE + smem_pos(k2)] = make_float2(x.x, x.y);
-        sm[rr * STRIDE + smem_pos(k2 + 1)] = make_float2(x.z, x.w);
+        sm[rr * STRIDE + ct_pos(k2)] = make_float2(x.x, x.y);
+        sm[rr * STRIDE + ct_pos(k2 + 1)] = make_float2(x.z, x.w);
     }
     double part = 0;
     const double* pp = a.partial + size_t(g) * a.partial_stride;
@@ -306,7 +322,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
                 const int rr = which == 0 ? 0 : R;
                 const uint32_t k = which == 0 ? L1 * k2 : L1 / 2 + L1 * k2;
                 const int m2 = which == 0 ? (L2 - k2) % L2 : L2 - 1 - k2;
-                const float2 zk = sm[rr * STRIDE + smem_pos(k2)], zm = sm[rr * STRIDE + smem_pos(m2)];
+                const float2 zk = sm[rr * STRIDE + ct_pos(k2)], zm = sm[rr * STRIDE + ct_pos(m2)];
                 float2 X;
                 if (k == 0) {
                     X = make_float2(zk.x + zk.y + pad0, 0.f);
@@ -329,7 +345,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             const uint32_t brow = L1 - arow;
             const uint32_t k = arow + L1 * k2;
             const uint32_t km = brow + L1 * uint32_t(L2 - 1 - k2);
-            const float2 zk = sm[r * STRIDE + smem_pos(k2)], zm = sm[(R + r) * STRIDE + smem_pos(L2 - 1 - k2)];
+            const float2 zk = sm[r * STRIDE + ct_pos(k2)], zm = sm[(R + r) * STRIDE + ct_pos(L2 - 1 - k2)];
             float sv, cv;
             sincospif(float(k) / fn, &sv, &cv);
             const float2 w = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, k);
