@@ -70,7 +70,7 @@ BANK_CANDIDATE = np.dtype([("power", "<f8"), ("period", "<f8"), ("tau", "<f8"), 
 
 OPT = dict(software=1, stockham=2, radix4=4, packed=8, scatter=16, radix8=32, fused_power=64, radix8_store=128,
            plain=1 << 16)
-STATUS_OVERFLOW, STATUS_RESAMPLE_OOB = 1, 2
+STATUS_OVERFLOW, STATUS_RESAMPLE_OOB, STATUS_MMA_TIMEOUT = 1, 2, 4
 FLAG_FMA, FLAG_INDEX_FP64 = 2, 256
 
 # Every symbol declared in include/brp_cuda.h.
@@ -152,7 +152,9 @@ def check(status, message_fn):
 
 
 def fast_configs():
-    """Compiled pass configurations: list of (id, L, kind) with kind 1 = pass 1, 2 = pass 2."""
+    """Compiled pass configurations: list of (id, L, kind) with kind 1 = pass 1,
+    2 = pass 2, 3 = pass 1 with its first radix-16 stage on the tensor cores
+    (chosen only by id)."""
     L = lib()
     n = L.brp_cuda_fast_configs(None, None, None, 0)
     ids = np.zeros(n, np.int32)

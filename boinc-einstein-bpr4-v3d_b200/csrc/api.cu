@@ -766,7 +766,7 @@ extern "C" int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* 
             if (k < cap) {
                 if (ids) ids[k] = f.id;
                 if (lengths) lengths[k] = f.L;
-                if (kinds) kinds[k] = uint32_t(kind);
+                if (kinds) kinds[k] = uint32_t(kind == 1 && f.tensor ? 3 : kind);
             }
             ++k;
         }

@@ -75,8 +75,13 @@ struct FastPass {
     cudaError_t (*attr)() = nullptr;
     RadixPlanHost plan;
     int table = 0;
+    int tensor = 0;  // pass 1 only: BF16 parts per operand of the tensor-core first stage (0: CUDA cores)
 };
+// Compiled pass configurations.  Pass-1 configurations with tensor != 0 (the
+// tensor-core form, fused_tc.cu) follow the CUDA-core ones and are chosen only
+// by id.
 const std::vector<FastPass>& fast_pass1_configs();
+void append_pass1_tc_configs(std::vector<FastPass>& v);
 const std::vector<FastPass>& fast_pass2_configs();
 size_t harmonic_fast_smem();
 cudaError_t set_harmonic_fast_attributes();

@@ -6,219 +6,10 @@
 // pass in registers.  Twiddles of a pass with span Ns and radix R come from a
 // per-pass table tw[k * RS + r - 1] = W_{Ns R}^{r k} (RS = R rounded up to even,
 // so pairs load as one 16-byte access).
-//
-// Resampling uses an instruction-lean form of the reference arithmetic that is
-// bit-identical to it (src/science.cpp:20-40, :80):
-//  * float(i) for i < 2^23 from the exponent trick 0x4B000000 | i;
-//  * the table index int(x) for x in [0.5, 64.5] and float(int(x)) from one
-//    add rounded toward -inf to 2^23 (its low mantissa bits are floor(x));
-//  * (int)((double)index + 0.5) as trunc(fl_toward_zero(index + 0.5)): with
-//    every integer below 2^24 representable, rounding toward zero never crosses
-//    an integer, so truncating the rounded sum equals truncating the exact one.
-// The reference-order function brp_resample_index (resample_math.h) remains the
-// definition; tests compare both against the CPU resampler bit for bit.
-#include "brp_internal.h"
-#include "fft_device.cuh"
-#include "resample_math.h"
+#include "fast_common.cuh"
 
 namespace brp {
-
-__constant__ uint32_t c_fast_lut_bits[130] = BRP_LUT_BITS;
-
 namespace {
-
-// Shared-memory layout of the compiled kernels: element e of a sequence at
-// e + e / 16 (one padding slot per 16 keeps radix-16 strided stores on distinct
-// banks).  Sequences sit `stride` elements apart, stride = 16/G (mod 16)
-// (G = sequences a warp touches side by side).
-__host__ __device__ constexpr int ct_pos(int e) { return e + (e >> 4); }
-__host__ __device__ constexpr int ct_stride(int L, int G) {
-    int base = L + L / 16;
-    int want = (G >= 16) ? 1 : 16 / G;
-    int pad = ((want - base) % 16 + 16) % 16;
-    return base + pad;
-}
-
-template <int R> struct TwStride { static constexpr int value = (R + 1) & ~1; };
-
-template <int R, int Ns>
-__device__ __forceinline__ void ct_twiddle(float2* v, const float2* __restrict__ tw, int k) {
-    if constexpr (Ns > 1) {
-        constexpr int RS = TwStride<R>::value;
-        const float4* w4 = reinterpret_cast<const float4*>(tw + k * RS);
-#pragma unroll
-        for (int r = 1; r < R; r += 2) {
-            const float4 w = __ldg(w4 + (r - 1) / 2);
-            v[r] = cmul(v[r], make_float2(w.x, w.y));
-            if (r + 1 < R) v[r + 1] = cmul(v[r + 1], make_float2(w.z, w.w));
-        }
-    }
-}
-
-// One Stockham pass: each thread loads its butterflies' inputs, the CTA
-// synchronises, then each thread twiddles, transforms and stores in place.
-template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
-__device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ tw) {
-    constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
-    float2 v[PER][R];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int b = threadIdx.x + q * THREADS;
-        if (TOTAL % THREADS == 0 || b < TOTAL) {
-            const int c = b / NBF, j = b - c * NBF;
-            const float2* src = buf + c * STRIDE;
-#pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = src[ct_pos(j + r * NBF)];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int b = threadIdx.x + q * THREADS;
-        if (TOTAL % THREADS == 0 || b < TOTAL) {
-            const int c = b / NBF, j = b - c * NBF;
-            const int k = j % Ns;
-            ct_twiddle<R, Ns>(v[q], tw, k);
-            dft<R>(v[q]);
-            float2* dst = buf + c * STRIDE;
-            const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) dst[ct_pos(base + r * Ns)] = v[q][r];
-        }
-    }
-    __syncthreads();
-}
-
-template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
-__device__ __forceinline__ void ct_fft(float2* buf, const float2* __restrict__ tw) {
-    ct_pass<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw);
-    if constexpr (sizeof...(Rest) > 0)
-        ct_fft<L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R>::value : 0));
-}
-
-// Number of float2 entries of the per-pass twiddle table of a radix sequence.
-template <int Ns, int R, int... Rest>
-__host__ __device__ constexpr int ct_table_size() {
-    int here = Ns > 1 ? Ns * TwStride<R>::value : 0;
-    if constexpr (sizeof...(Rest) > 0) return here + ct_table_size<Ns * R, Rest...>();
-    else return here;
-}
-
-// ---- bit-identical lean resampling index (see the file comment) ----
-__device__ __forceinline__ float u2f_exact(uint32_t i) {
-    return i < (1u << 23) ? __fsub_rn(__int_as_float(0x4B000000 | int(i)), 8388608.0f) : __uint2float_rn(i);
-}
-
-template <bool FMA>
-__device__ __forceinline__ int lean_index(uint32_t i, const brp_resample_consts& p) {
-    const float fi = u2f_exact(i);
-    const float t = __fmul_rn(fi, p.dt);
-    const float ph = FMA ? __fmaf_rn(p.omega, t, p.psi) : __fadd_rn(__fmul_rn(p.omega, t), p.psi);
-    const float y = __fmul_rn(BRP_INV_TWO_PI_F, ph);
-    float xt = __fsub_rn(y, truncf(y));
-    if (xt < 0.f) xt = __fadd_rn(xt, 1.0f);
-    const float x64 = FMA ? __fmaf_rn(xt, 64.0f, 0.5f) : __fadd_rn(__fmul_rn(xt, 64.0f), 0.5f);
-    const float mg = __fadd_rd(x64, 8388608.0f);
-    const int li = __float_as_int(mg) - 0x4B000000;
-    const float fli = __fsub_rn(mg, 8388608.0f);
-    const float s = __uint_as_float(c_fast_lut_bits[2 * li]), c = __uint_as_float(c_fast_lut_bits[2 * li + 1]);
-    float sn, off;
-    if (FMA) {
-        const float d = __fmul_rn(BRP_TWO_PI_F, __fmaf_rn(-fli, 0.015625f, xt));
-        const float d2 = __fmul_rn(__fmul_rn(0.5f, d), d);
-        sn = __fmaf_rn(-d2, s, __fmaf_rn(d, c, s));
-        off = __fmaf_rn(__fmul_rn(p.tau, sn), p.step_inv, -p.s0);
-    } else {
-        const float d = __fmul_rn(BRP_TWO_PI_F, __fsub_rn(xt, __fmul_rn(0.015625f, fli)));
-        const float d2 = __fmul_rn(d, __fmul_rn(0.5f, d));
-        sn = __fsub_rn(__fadd_rn(s, __fmul_rn(d, c)), __fmul_rn(d2, s));
-        off = __fsub_rn(__fmul_rn(__fmul_rn(p.tau, sn), p.step_inv), p.s0);
-    }
-    const float index = __fsub_rn(fi, off);
-    return __float2int_rz(__fadd_rz(index, 0.5f));
-}
-
-__device__ __forceinline__ brp_resample_consts consts_of(const brp_params& p) {
-    brp_resample_consts c;
-    c.tau = p.tau; c.omega = p.omega; c.psi = p.psi; c.dt = p.dt; c.step_inv = p.step_inv; c.s0 = p.s0;
-    c.flags = p.flags;
-    return c;
-}
-
-template <int THREADS>
-__device__ __forceinline__ double block_sum_d(double v, double* scratch) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) scratch[warp] = v;
-    __syncthreads();
-    double r = 0;
-    if (warp == 0) {
-        r = lane < THREADS / 32 ? scratch[lane] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-    }
-    return r;
-}
-
-// Gathers this CTA's samples (rows n1 < L1, C complex points = 2C consecutive
-// reals per row) into shared memory; returns the sum of the samples (FP32 per
-// thread, a few dozen samples, then FP64 across threads).  Thread t handles
-// column t % C of rows t / C + q THREADS / C: the two samples of a complex
-// point, one 64-bit store; sample index and shared address advance by
-// constants.
-template <int L1, int C, int THREADS, int STRIDE, int MODE>
-__device__ __forceinline__ double gather(float2* sm, const float* __restrict__ in, const brp_params& P,
-                                         uint32_t L2, uint32_t c0, float* raw, bool& oob) {
-    constexpr int TOTAL = L1 * C, PER = TOTAL / THREADS, ROWS_STEP = THREADS / C;
-    static_assert(TOTAL % THREADS == 0 && THREADS % C == 0, "gather must tile the CTA");
-    static_assert(ROWS_STEP % 16 == 0, "row step must keep the shared-memory padding periodic");
-    const brp_resample_consts rc = consts_of(P);
-    const uint32_t steps = P.steps, unpadded = P.unpadded;
-    const int c = threadIdx.x % C, n1_0 = threadIdx.x / C;
-    const uint32_t istep = 2u * L2 * ROWS_STEP;
-    uint32_t i = 2u * (L2 * uint32_t(n1_0) + c0 + uint32_t(c));
-    float2* dst = sm + c * STRIDE + ct_pos(n1_0);
-    constexpr int DSTEP = ROWS_STEP + (ROWS_STEP / 16);
-    float sum = 0.f;
-    // Indices of a batch of points first, then all of the batch's loads, so each
-    // thread keeps 2 BATCH gathers in flight.
-    constexpr int BATCH = 4;
-    static_assert(PER % BATCH == 0, "batch must divide the points per thread");
-#pragma unroll 1
-    for (int q0 = 0; q0 < PER; q0 += BATCH) {
-        int j[2 * BATCH];
-#pragma unroll
-        for (int b = 0; b < 2 * BATCH; ++b) {
-            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
-            j[b] = -1;
-            if (ib < steps) {
-                int jj;
-                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<MODE == 1>(ib, rc);
-                if (uint32_t(jj) < unpadded) j[b] = jj;
-                else oob = true;
-            }
-        }
-        float v[2 * BATCH];
-#pragma unroll
-        for (int b = 0; b < 2 * BATCH; ++b) v[b] = j[b] >= 0 ? __ldg(in + j[b]) : 0.f;
-#pragma unroll
-        for (int b = 0; b < BATCH; ++b) {
-            if (raw) {
-                const uint32_t ib = i + uint32_t(b) * istep;
-                if (ib < steps) raw[ib] = v[2 * b];
-                if (ib + 1 < steps) raw[ib + 1] = v[2 * b + 1];
-            }
-            sum += v[2 * b];
-            sum += v[2 * b + 1];
-            dst[b * DSTEP] = make_float2(v[2 * b], v[2 * b + 1]);
-        }
-        i += BATCH * istep;
-        dst += BATCH * DSTEP;
-    }
-    return double(sum);
-}
 
 template <int L1, int C, int THREADS, int MINB, int... Rs>
 __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
@@ -410,8 +201,8 @@ struct P2 {
 
 }  // namespace
 
-const std::vector<FastPass>& fast_pass1_configs() {
-    static const std::vector<FastPass> v = {
+static std::vector<FastPass> make_pass1_configs() {
+    std::vector<FastPass> v = {
         P1<2048, 4, 512, 2, 16, 16, 8>::info(101),
         P1<2048, 2, 256, 4, 16, 16, 8>::info(102),
         P1<1024, 4, 256, 4, 16, 8, 8>::info(103),
@@ -420,6 +211,12 @@ const std::vector<FastPass>& fast_pass1_configs() {
         P1<3072, 2, 384, 2, 16, 16, 4, 3>::info(106),
         P1<512, 8, 256, 4, 8, 8, 8>::info(107),
     };
+    append_pass1_tc_configs(v);
+    return v;
+}
+
+const std::vector<FastPass>& fast_pass1_configs() {
+    static const std::vector<FastPass> v = make_pass1_configs();
     return v;
 }
 

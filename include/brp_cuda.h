@@ -32,8 +32,10 @@ extern "C" {
 enum { BRP_OK = 0, BRP_E_RUNTIME = 1, BRP_E_RESULT = 2, BRP_E_TIMEOUT = 3, BRP_E_ARGUMENT = 4 };
 
 /* Per-template device error word bits (shaders/resample.comp:18,
- * shaders/harmonic.comp:34). */
-enum { BRP_STATUS_OVERFLOW = 1u, BRP_STATUS_RESAMPLE_OOB = 2u };
+ * shaders/harmonic.comp:34).  BRP_STATUS_MMA_TIMEOUT has no reference
+ * counterpart: the tensor-core pass-1 form (compiled pass-1 configurations
+ * 111-114) gave up waiting for its matrix multiplies. */
+enum { BRP_STATUS_OVERFLOW = 1u, BRP_STATUS_RESAMPLE_OOB = 2u, BRP_STATUS_MMA_TIMEOUT = 4u };
 
 /* Byte-identical to brp::Params (include/brp/science.hpp:8-17, 108 bytes). */
 typedef struct brp_params {
@@ -142,7 +144,9 @@ int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_
 int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
                             uint32_t chains);
 /* Lists the compiled configurations: ids, sequence length L (pass 1: column
- * length L1, pass 2: row length L2) and kind (1 = pass 1, 2 = pass 2).
+ * length L1, pass 2: row length L2) and kind (1 = pass 1, 2 = pass 2,
+ * 3 = pass 1 whose first radix-16 stage runs on the tensor cores as split
+ * BF16 DFT products; kind 3 is never a default and is selected by id).
  * Returns the total count; writes at most cap entries. */
 int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* kinds, uint32_t cap);
 /* Device-only replay of the last brp_cuda_bank_run's graph (no host copies,

@@ -67,3 +67,15 @@ def test_oracle_library_exports():
     for name in ("oracle_resample", "oracle_harmonic", "oracle_select", "oracle_search_parameters",
                  "oracle_toplist_retain", "oracle_toplist_final", "oracle_rfft64"):
         assert hasattr(L, name)
+
+
+def test_tensor_core_pass1_configs_listed():
+    """The tensor-core pass-1 forms (kind 3) sit beside the CUDA-core pass-1
+    configuration of the same column length and never enter the autotuner."""
+    from brp_b200 import tune
+    from brp_b200._lib import fast_configs
+    kinds = {i: (L, k) for i, L, k in fast_configs()}
+    for tc, base in ((111, 101), (112, 101), (113, 106), (114, 106)):
+        assert kinds[tc] == (kinds[base][0], 3)
+    ids = {c[0] for c in tune.candidates(1 << 22) + tune.candidates(3 << 21)}
+    assert ids and not ids & {111, 112, 113, 114}
