@@ -215,5 +215,84 @@ __device__ __forceinline__ double gather(float2* sm, const float* __restrict__ i
     return double(sum);
 }
 
+// Gather fused with the first Stockham pass (span 1, radix 16) when each
+// thread owns exactly one of its butterflies (L1 C = 16 THREADS): thread
+// t = j C + c gathers the 16 points n1 = j + r L1/16 of column c (the same
+// points, sums and snapshot writes as gather), transforms them in registers and
+// stores the 16 outputs at 16 j + m, so the samples never take a shared-memory
+// round trip before the first pass.
+template <int L1, int C, int THREADS, int STRIDE, int MODE>
+__device__ __forceinline__ double gather_dft16(float2* sm, const float* __restrict__ in, const brp_params& P,
+                                               uint32_t L2, uint32_t c0, float* raw, bool& oob) {
+    constexpr int NBF = L1 / 16;
+    static_assert(L1 * C == 16 * THREADS, "one first-pass butterfly per thread");
+    const brp_resample_consts rc = consts_of(P);
+    const uint32_t steps = P.steps, unpadded = P.unpadded;
+    const int t = threadIdx.x, c = t % C, j = t / C;
+    const uint32_t istep = 2u * L2 * uint32_t(NBF);
+    uint32_t i = 2u * (L2 * uint32_t(j) + c0 + uint32_t(c));
+    float2 x[16];
+    float sum = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        int jx[8];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
+            jx[b] = -1;
+            if (ib < steps) {
+                int jj;
+                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
+                else jj = lean_index<MODE == 1>(ib, rc);
+                if (uint32_t(jj) < unpadded) jx[b] = jj;
+                else oob = true;
+            }
+        }
+        float v[8];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) v[b] = jx[b] >= 0 ? __ldg(in + jx[b]) : 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            if (raw) {
+                const uint32_t ib = i + uint32_t(b) * istep;
+                if (ib < steps) raw[ib] = v[2 * b];
+                if (ib + 1 < steps) raw[ib + 1] = v[2 * b + 1];
+            }
+            sum += v[2 * b];
+            sum += v[2 * b + 1];
+            x[4 * q + b] = make_float2(v[2 * b], v[2 * b + 1]);
+        }
+        i += 4u * istep;
+    }
+    dft16(x);
+    float2* dst = sm + c * STRIDE + ct_pos(16 * j);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) dst[m] = x[m];
+    return double(sum);
+}
+
+// Four-step twiddle and store of the transformed columns: T[k1][c0 + c] =
+// Y[c][k1] W_M^{(c0 + c) k1}.  Thread t keeps column c = t % C and visits rows
+// k1 = t / C + it THREADS / C; the twiddle comes from the two-level table at
+// every fourth row and in between from the product with W_M^{(c0 + c) THREADS / C}
+// (at most three FP32 complex products from a table value).
+template <int L1, int C, int THREADS, int STRIDE>
+__device__ __forceinline__ void store_twiddled(const float2* sm, float2* __restrict__ T, const float2* fs_hi,
+                                               const float2* fs_lo, uint32_t L2, uint32_t c0) {
+    constexpr int ITER = L1 * C / THREADS, KSTEP = THREADS / C;
+    static_assert(THREADS % C == 0 && (L1 * C) % THREADS == 0, "store tiling");
+    const int c = threadIdx.x % C, k1_0 = threadIdx.x / C;
+    const uint32_t n2 = c0 + uint32_t(c);
+    const float2 step = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(KSTEP));
+    float2 w;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int k1 = k1_0 + it * KSTEP;
+        if (it % 4 == 0) w = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(k1));
+        else w = cmul(w, step);
+        T[size_t(k1) * L2 + n2] = cmul(sm[c * STRIDE + ct_pos(k1)], w);
+    }
+}
+
 }  // namespace
 }  // namespace brp

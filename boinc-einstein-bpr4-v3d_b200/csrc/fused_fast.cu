@@ -5,15 +5,18 @@
 // immediate offsets, and each thread holds exactly one butterfly's inputs per
 // pass in registers.  Twiddles of a pass with span Ns and radix R come from a
 // per-pass table tw[k * RS + r - 1] = W_{Ns R}^{r k} (RS = R rounded up to even,
-// so pairs load as one 16-byte access).
+// so pairs load as one 16-byte access).  Where a pass-1 thread owns exactly one
+// radix-16 butterfly of the first pass, that pass runs in registers inside the
+// gather (gather_dft16), one shared-memory round trip and barrier fewer.
 #include "fast_common.cuh"
 
 namespace brp {
 namespace {
 
-template <int L1, int C, int THREADS, int MINB, int... Rs>
+template <int L1, int C, int THREADS, int MINB, int R0, int... Rest>
 __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     constexpr int STRIDE = ct_stride(L1, C);
+    constexpr bool FIRST = R0 == 16 && L1 * C == 16 * THREADS;  // first pass fused into the gather
     extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[THREADS / 32];
     const int g = blockIdx.y;
@@ -23,25 +26,25 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     float* raw = (g == a.snap) ? a.snap_raw : nullptr;
     bool oob = false;
     double sum;
-    if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
-    else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
-    else sum = gather<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
+    if constexpr (FIRST) {
+        if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather_dft16<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
+        else if (P.flags & 2u) sum = gather_dft16<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
+        else sum = gather_dft16<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
+    } else {
+        if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
+        else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
+        else sum = gather<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
+    }
     if (oob) atomicOr(a.status + g, BRP_STATUS_RESAMPLE_OOB);
     const double tot = block_sum_d<THREADS>(sum, red);
     if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
     __syncthreads();
 
-    ct_fft<L1, STRIDE, C, THREADS, 1, Rs...>(sm, a.ptw1);
+    if constexpr (FIRST) ct_fft<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1);
+    else ct_fft<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1);
 
     float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < L1 * C; idx += THREADS) {
-        const int k1 = idx / C, c = idx % C;
-        float2 y = sm[c * STRIDE + ct_pos(k1)];
-        const uint32_t e = (c0 + uint32_t(c)) * uint32_t(k1);
-        y = cmul(y, twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, e));
-        T[size_t(k1) * L2 + c0 + c] = y;
-    }
+    store_twiddled<L1, C, THREADS, STRIDE>(sm, T, a.fs_hi, a.fs_lo, L2, c0);
 }
 
 __device__ __forceinline__ uint32_t mod_n(uint64_t x, uint32_t n) {

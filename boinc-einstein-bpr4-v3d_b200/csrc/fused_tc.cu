@@ -314,15 +314,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
 
     ct_fft<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1);
 
-    float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < L1 * C; idx += THREADS) {
-        const int k1 = idx / C, c = idx % C;
-        float2 y = sm[c * STRIDE + ct_pos(k1)];
-        const uint32_t e = (c0 + uint32_t(c)) * uint32_t(k1);
-        y = cmul(y, twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, e));
-        T[size_t(k1) * L2 + c0 + c] = y;
-    }
+    store_twiddled<L1, C, THREADS, STRIDE>(sm, a.work + size_t(g) * a.work_stride, a.fs_hi, a.fs_lo, L2, c0);
 }
 
 template <int L1, int C, int THREADS, int MINB, int TERMS, int... Rest>
