@@ -60,9 +60,19 @@ __device__ __forceinline__ float2 real_bin(float2 zk, float2 zm, float2 w, float
     return make_float2(0.5f * (s.x + t.y) + pad.x, 0.5f * (s.y - t.x) + pad.y);
 }
 
-template <int L2, int R, int THREADS, int MINB, int... Rs>
+// Row of sequence rr of pass-2 CTA q: rows [0, R) are qR + r, rows [R, 2R) their
+// mirrors L1 - (qR + r), with row L1/2 in place of row 0's mirror.
+__device__ __forceinline__ uint32_t pass2_row(int rr, int R, uint32_t q, uint32_t L1) {
+    if (rr < R) return q * R + rr;
+    const uint32_t ar = q * R + (rr - R);
+    return ar == 0 ? L1 / 2 : L1 - ar;
+}
+
+template <int L2, int R, int THREADS, int MINB, int R0, int... Rest>
 __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     constexpr int SEQ = 2 * R, STRIDE = ct_stride(L2, R);
+    // first pass (radix 16) fused into the row loads when each thread owns one of its butterflies
+    constexpr bool FIRST = R0 == 16 && SEQ * L2 == 16 * THREADS;
     extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[THREADS / 32];
     __shared__ float s_mean;
@@ -71,19 +81,26 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     const uint32_t L1 = a.L1, n = a.n, M = a.M, steps = P.steps;
     const float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
 
-    // rows [0, R): qR + r; rows [R, 2R): L1 - (qR + r), row L1/2 in place of row 0's mirror
+    if constexpr (FIRST) {
+        // thread t: sequence t / (L2/16), butterfly j = t % (L2/16), inputs j + r L2/16
+        constexpr int NBF = L2 / 16;
+        const int rr = threadIdx.x / NBF, j = threadIdx.x % NBF;
+        const float2* src = T + size_t(pass2_row(rr, R, q, L1)) * L2 + j;
+        float2 x[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) x[r] = __ldg(src + r * NBF);
+        dft16(x);
+        float2* dst = sm + rr * STRIDE + ct_pos(16 * j);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) dst[m] = x[m];
+    } else {
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < SEQ * L2 / 2; idx += THREADS) {
-        const int rr = idx / (L2 / 2), k2 = 2 * (idx % (L2 / 2));
-        uint32_t row;
-        if (rr < R) row = q * R + rr;
-        else {
-            const uint32_t ar = q * R + (rr - R);
-            row = ar == 0 ? L1 / 2 : L1 - ar;
+        for (int idx = threadIdx.x; idx < SEQ * L2 / 2; idx += THREADS) {
+            const int rr = idx / (L2 / 2), k2 = 2 * (idx % (L2 / 2));
+            const float4 x = __ldg(reinterpret_cast<const float4*>(T + size_t(pass2_row(rr, R, q, L1)) * L2 + k2));
+            sm[rr * STRIDE + ct_pos(k2)] = make_float2(x.x, x.y);
+            sm[rr * STRIDE + ct_pos(k2 + 1)] = make_float2(x.z, x.w);
         }
-        const float4 x = __ldg(reinterpret_cast<const float4*>(T + size_t(row) * L2 + k2));
-        sm[rr * STRIDE + ct_pos(k2)] = make_float2(x.x, x.y);
-        sm[rr * STRIDE + ct_pos(k2 + 1)] = make_float2(x.z, x.w);
     }
     double part = 0;
     const double* pp = a.partial + size_t(g) * a.partial_stride;
@@ -97,7 +114,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     __syncthreads();
     const float mean = s_mean;
 
-    ct_fft<L2, STRIDE, SEQ, THREADS, 1, Rs...>(sm, a.ptw2);
+    if constexpr (FIRST) ct_fft<L2, STRIDE, SEQ, THREADS, 16, Rest...>(sm, a.ptw2);
+    else ct_fft<L2, STRIDE, SEQ, THREADS, 1, R0, Rest...>(sm, a.ptw2);
 
     float* __restrict__ Pw = a.power + size_t(g) * a.power_stride;
     float2* fft = (g == a.snap) ? a.snap_fft : nullptr;
@@ -106,10 +124,19 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     const bool a_odd = steps & 1u;
     const float pad0 = float(n - steps) * mean;
 
+    // Thread t keeps row pair r = t % R and visits k2 = t / R + it THREADS / R,
+    // so k = qR + r + L1 k2 advances by L1 THREADS / R: W_n^{k steps} comes from
+    // the two-level table at every fourth bin and in between from the product
+    // with W_n^{L1 (THREADS / R) steps}.
+    static_assert(THREADS % R == 0 && (R * L2) % THREADS == 0, "post-processing tiling");
+    constexpr int ITER = R * L2 / THREADS, KSTEP = THREADS / R;
+    const int r = threadIdx.x % R;
+    const uint32_t arow = q * R + r;
+    const float2 wa_step = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(L1) * KSTEP * steps, n));
+    float2 wa;
 #pragma unroll 2
-    for (int idx = threadIdx.x; idx < R * L2; idx += THREADS) {
-        const int r = idx % R, k2 = idx / R;
-        const uint32_t arow = q * R + r;
+    for (int it = 0; it < ITER; ++it) {
+        const int k2 = threadIdx.x / R + it * KSTEP;
         if (arow == 0) {
 #pragma unroll
             for (int which = 0; which < 2; ++which) {
@@ -126,8 +153,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
                     const float2 hf = twiddle2(a.hf_hi, a.hf_lo, kSplitLog2, k);
                     const float cv = hf.x, sv = -hf.y;
                     const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
-                    const float2 wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
-                    const float2 G = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
+                    const float2 wk = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+                    const float2 G = cmul(make_float2(1.f - wk.x, -wk.y), make_float2(sv, -cv));
                     const float f = __fdividef(-0.5f * mean, sv);
                     X = real_bin(zk, zm, w, make_float2(G.x * f, G.y * f));
                     const float pw = X.x * X.x + X.y * X.y;
@@ -140,10 +167,12 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             const uint32_t k = arow + L1 * k2;
             const uint32_t km = brow + L1 * uint32_t(L2 - 1 - k2);
             const float2 zk = sm[r * STRIDE + ct_pos(k2)], zm = sm[(R + r) * STRIDE + ct_pos(L2 - 1 - k2)];
-            float sv, cv;
-            sincospif(float(k) / fn, &sv, &cv);
-            const float2 w = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, k);
-            const float2 wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+            // cos, sin of pi k / n from the W_2n table; W_n^k = (cos - i sin)^2
+            const float2 hf = twiddle2(a.hf_hi, a.hf_lo, kSplitLog2, k);
+            const float cv = hf.x, sv = -hf.y;
+            const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
+            if (it % 4 == 0) wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+            else wa = cmul(wa, wa_step);
             const float2 wm = make_float2(-w.x, w.y);
             const float2 wam = a_odd ? make_float2(-wa.x, wa.y) : make_float2(wa.x, -wa.y);
             const float2 G1 = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));

@@ -220,32 +220,39 @@ void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
 
 // Gathers the candidates of `count` result slots back to back:
 // offsets[t] = sum of min(counts[u], capacity) for u < t, offsets[count] = total.
-__global__ void bank_compact_kernel(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity,
-                                    uint32_t count, brp_candidate* out, uint64_t out_cap, uint64_t* offsets) {
-    __shared__ uint64_t s_off;
-    // Serial prefix by one thread (count is at most a few thousand).
-    if (threadIdx.x == 0) {
-        uint64_t acc = 0;
-        for (uint32_t t = 0; t < count; ++t) {
-            offsets[t] = acc;
-            acc += counts[t] < capacity ? counts[t] : capacity;
-        }
-        offsets[count] = acc;
-    }
+// One CTA per slot: it sums the clamped counts before its slot (a CTA-wide
+// reduction; count is at most a few thousand) and copies its slot's
+// candidates, 16 bytes per thread.
+static_assert(sizeof(brp_candidate) == 16, "candidates move as 16-byte vectors");
+
+__global__ void __launch_bounds__(256) bank_compact_kernel(const uint32_t* counts, const brp_candidate* cands,
+                                                           uint32_t capacity, uint32_t count, brp_candidate* out,
+                                                           uint64_t out_cap, uint64_t* offsets) {
+    __shared__ uint64_t s_part[8];
+    const uint32_t t = blockIdx.x;
+    uint64_t acc = 0;
+    for (uint32_t u = threadIdx.x; u < t; u += blockDim.x) acc += min(counts[u], capacity);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
     __syncthreads();
-    for (uint32_t t = blockIdx.x; t < count; t += gridDim.x) {
-        if (threadIdx.x == 0) s_off = offsets[t];
-        __syncthreads();
-        const uint32_t c = counts[t] < capacity ? counts[t] : capacity;
-        for (uint32_t k = threadIdx.x; k < c; k += blockDim.x)
-            if (s_off + k < out_cap) out[s_off + k] = cands[size_t(t) * capacity + k];
-        __syncthreads();
+    uint64_t off = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) off += s_part[w];
+    const uint32_t c = min(counts[t], capacity);
+    if (threadIdx.x == 0) {
+        offsets[t] = off;
+        if (t + 1 == count) offsets[count] = off + c;
     }
+    const uint4* src = reinterpret_cast<const uint4*>(cands + size_t(t) * capacity);
+    uint4* dst = reinterpret_cast<uint4*>(out);
+    for (uint32_t k = threadIdx.x; k < c; k += blockDim.x)
+        if (off + k < out_cap) dst[off + k] = src[k];
 }
 
 void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
                          brp_candidate* out, uint64_t out_cap, uint64_t* offsets, cudaStream_t s) {
-    bank_compact_kernel<<<1, 256, 0, s>>>(counts, cands, capacity, count, out, out_cap, offsets);
+    if (count) bank_compact_kernel<<<count, 256, 0, s>>>(counts, cands, capacity, count, out, out_cap, offsets);
 }
 
 }  // namespace brp
