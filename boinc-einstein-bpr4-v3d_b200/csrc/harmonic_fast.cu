@@ -248,7 +248,9 @@ __device__ __forceinline__ void sums_and_levels(const HCtx& c, LevelTail (&head)
                          head[3], tail[3]);
 }
 
-__global__ void __launch_bounds__(kHThreads) harmonic_fast_kernel(FusedArgs a) {
+// Six CTAs per SM (80 registers per thread): the shared-memory staging allows
+// six, and the extra warps hide the latency of the direct global loads.
+__global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a) {
     extern __shared__ __align__(16) float stage[];
     __shared__ float xwarp[kHThreads / 32][8];
     __shared__ int doff[8];
