@@ -271,26 +271,53 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
     return double(sum);
 }
 
-// Four-step twiddle and store of the transformed columns: T[k1][c0 + c] =
-// Y[c][k1] W_M^{(c0 + c) k1}.  Thread t keeps column c = t % C and visits rows
-// k1 = t / C + it THREADS / C; the twiddle comes from the two-level table at
-// every fourth row and in between from the product with W_M^{(c0 + c) THREADS / C}
-// (at most three FP32 complex products from a table value).
-template <int L1, int C, int THREADS, int STRIDE>
-__device__ __forceinline__ void store_twiddled(const float2* sm, float2* __restrict__ T, const float2* fs_hi,
-                                               const float2* fs_lo, uint32_t L2, uint32_t c0) {
-    constexpr int ITER = L1 * C / THREADS, KSTEP = THREADS / C;
-    static_assert(THREADS % C == 0 && (L1 * C) % THREADS == 0, "store tiling");
-    const int c = threadIdx.x % C, k1_0 = threadIdx.x / C;
+// Last Stockham pass of pass 1 (span Ns, radix R, Ns R = L) fused with the
+// four-step twiddle and the store of the transformed columns:
+//     T[k1][c0 + c] = Y[c][k1] W_M^{(c0 + c) k1}.
+// Butterfly b of the pass takes column c = b % SEQ and j = b / SEQ, so a warp
+// stores 32/SEQ rows of SEQ adjacent columns; its outputs are rows k1 = j + m Ns.
+// The twiddle comes from the two-level table for m = 0 and m = 4 and in
+// between from the product with W_M^{(c0 + c) Ns} (at most three FP32 complex
+// products from a table value).
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
+__device__ __forceinline__ void ct_last_pass_store(const float2* buf, const float2* __restrict__ tw,
+                                                   float2* __restrict__ T, const float2* fs_hi, const float2* fs_lo,
+                                                   uint32_t L2, uint32_t c0) {
+    constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
+    static_assert(Ns * R == L && THREADS % SEQ == 0, "last-pass tiling");
+    const int c = threadIdx.x % SEQ;
     const uint32_t n2 = c0 + uint32_t(c);
-    const float2 step = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(KSTEP));
-    float2 w;
+    const float2 step = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(Ns));
+    const float2* src = buf + c * STRIDE;
 #pragma unroll
-    for (int it = 0; it < ITER; ++it) {
-        const int k1 = k1_0 + it * KSTEP;
-        if (it % 4 == 0) w = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(k1));
-        else w = cmul(w, step);
-        T[size_t(k1) * L2 + n2] = cmul(sm[c * STRIDE + ct_pos(k1)], w);
+    for (int q = 0; q < PER; ++q) {
+        if (TOTAL % THREADS != 0 && threadIdx.x + q * THREADS >= TOTAL) break;
+        const int j = threadIdx.x / SEQ + q * (THREADS / SEQ);
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[ct_pos(j + r * NBF)];
+        ct_twiddle<R, Ns>(v, tw, j);
+        dft<R>(v);
+        float2 w;
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            if (m % 4 == 0) w = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(j + m * Ns));
+            else w = cmul(w, step);
+            T[size_t(j + m * Ns) * L2 + n2] = cmul(v[m], w);
+        }
+    }
+}
+
+// The shared-memory passes of pass 1 with the last one fused with the store.
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
+__device__ __forceinline__ void ct_fft_store(float2* buf, const float2* __restrict__ tw, float2* __restrict__ T,
+                                             const float2* fs_hi, const float2* fs_lo, uint32_t L2, uint32_t c0) {
+    if constexpr (sizeof...(Rest) == 0) {
+        ct_last_pass_store<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw, T, fs_hi, fs_lo, L2, c0);
+    } else {
+        ct_pass<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw);
+        ct_fft_store<L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R>::value : 0), T,
+                                                              fs_hi, fs_lo, L2, c0);
     }
 }
 

@@ -40,11 +40,9 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
     __syncthreads();
 
-    if constexpr (FIRST) ct_fft<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1);
-    else ct_fft<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1);
-
     float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
-    store_twiddled<L1, C, THREADS, STRIDE>(sm, T, a.fs_hi, a.fs_lo, L2, c0);
+    if constexpr (FIRST) ct_fft_store<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
+    else ct_fft_store<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
 }
 
 __device__ __forceinline__ uint32_t mod_n(uint64_t x, uint32_t n) {

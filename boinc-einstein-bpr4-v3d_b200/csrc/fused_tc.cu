@@ -1,8 +1,8 @@
 // Tensor-core form of the fused pass 1: the first radix-16 stage of the column
 // FFTs runs as a matrix product on the fifth-generation tensor cores
 // (tcgen05.mma kind::f16, BF16 operands, FP32 accumulation in tensor memory);
-// the remaining Stockham passes, the four-step twiddle and the store are those
-// of pass1_fast (fused_fast.cu).
+// the remaining Stockham passes, the last one fused with the four-step twiddle
+// and the store, are those of pass1_fast (fused_fast.cu).
 //
 // A CTA transforms C columns of L1 points.  The first Stockham pass (span 1,
 // radix 16) of a column is L1/16 independent 16-point DFTs: butterfly j takes
@@ -312,9 +312,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
         return;
     }
 
-    ct_fft<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1);
-
-    store_twiddled<L1, C, THREADS, STRIDE>(sm, a.work + size_t(g) * a.work_stride, a.fs_hi, a.fs_lo, L2, c0);
+    ct_fft_store<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, a.work + size_t(g) * a.work_stride, a.fs_hi, a.fs_lo,
+                                                    L2, c0);
 }
 
 template <int L1, int C, int THREADS, int MINB, int TERMS, int... Rest>
