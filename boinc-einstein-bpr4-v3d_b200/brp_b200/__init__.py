@@ -7,7 +7,7 @@ reference's brp::GPU, ``Bank`` runs a whole orbital bank in one CUDA graph,
 ``host`` holds the reference's host functions (template constants, search
 parameters, toplist), ``synth`` the seeded synthetic workloads.
 """
-from ._lib import (BANK_CANDIDATE, CANDIDATE, EXPORTS, BrpError, Params, STATUS_MMA_TIMEOUT, STATUS_OVERFLOW,
+from ._lib import (BANK_CANDIDATE, CANDIDATE, EXPORTS, BrpError, Params, STATUS_WAIT_TIMEOUT, STATUS_OVERFLOW,
                    STATUS_RESAMPLE_OOB, build, lib)
 from .bank import Bank
 from .gpu import GPU, Snapshot
@@ -15,4 +15,4 @@ from .host import Toplist, parameters, production, resampling_steps, search_para
 
 __all__ = ["GPU", "Bank", "Snapshot", "Params", "Toplist", "BrpError", "parameters", "production",
            "resampling_steps", "search_parameters", "build", "lib", "CANDIDATE", "BANK_CANDIDATE", "EXPORTS",
-           "STATUS_OVERFLOW", "STATUS_RESAMPLE_OOB", "STATUS_MMA_TIMEOUT"]
+           "STATUS_OVERFLOW", "STATUS_RESAMPLE_OOB", "STATUS_WAIT_TIMEOUT"]

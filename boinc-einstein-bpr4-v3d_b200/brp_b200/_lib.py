@@ -70,7 +70,7 @@ BANK_CANDIDATE = np.dtype([("power", "<f8"), ("period", "<f8"), ("tau", "<f8"), 
 
 OPT = dict(software=1, stockham=2, radix4=4, packed=8, scatter=16, radix8=32, fused_power=64, radix8_store=128,
            plain=1 << 16)
-STATUS_OVERFLOW, STATUS_RESAMPLE_OOB, STATUS_MMA_TIMEOUT = 1, 2, 4
+STATUS_OVERFLOW, STATUS_RESAMPLE_OOB, STATUS_WAIT_TIMEOUT = 1, 2, 4
 FLAG_FMA, FLAG_INDEX_FP64 = 2, 256
 
 # Every symbol declared in include/brp_cuda.h.

@@ -34,9 +34,10 @@
 // 32 FP32 per thread) and stores the 16 complex outputs into the padded FP32
 // layout of the CUDA-core passes, which overlays the operand tiles (the MMAs
 // have completed when the mbarrier phase flips).  A wait that reaches its
-// bound sets BRP_STATUS_MMA_TIMEOUT for the template, frees the tensor memory
+// bound sets BRP_STATUS_WAIT_TIMEOUT for the template, frees the tensor memory
 // and leaves the CTA.
 #include <cuda_bf16.h>
+#include "async_device.cuh"
 #include "fast_common.cuh"
 
 namespace brp {
@@ -46,10 +47,6 @@ constexpr int kTileRows = 128;              // MMA M
 constexpr int kTileBytes = kTileRows * 64;  // 128 rows x 32 BF16
 constexpr int kFBytes = 32 * 64;            // F: 32 rows x 32 BF16
 constexpr int kSmPerSm = 233472;            // shared memory of one SM (228 KiB)
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // Shared-memory matrix descriptor, K-major, no swizzle: start address, leading
 // byte offset 128, stride byte offset 512 (all in 16-byte units), version 1.
@@ -71,22 +68,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t 
         :
         : "r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
         : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 22); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (it >= 64) __nanosleep(128);
-    }
-    return false;
 }
 
 // Part products X_i F_j (i + j < terms), smallest first: (1,1) (0,2) (2,0)
@@ -237,8 +218,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init(bar, 1);
     }
     fill_dft16_operand<THREADS, TERMS>(Fm);
 
@@ -308,7 +288,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
                      : "memory");
     }
     if (timed_out) {
-        if (threadIdx.x == 0) atomicOr(a.status + g, BRP_STATUS_MMA_TIMEOUT);
+        if (threadIdx.x == 0) atomicOr(a.status + g, BRP_STATUS_WAIT_TIMEOUT);
         return;
     }
 

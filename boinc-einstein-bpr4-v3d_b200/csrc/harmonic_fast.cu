@@ -23,6 +23,7 @@
 // previous thread's last bins, whose maximum and first value arrive by warp
 // shuffle (and through shared memory across warps).  Thread 0 of each CTA only
 // computes that halo for thread 1.
+#include "async_device.cuh"
 #include "brp_internal.h"
 
 namespace brp {
@@ -254,6 +255,7 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     extern __shared__ __align__(16) float stage[];
     __shared__ float xwarp[kHThreads / 32][8];
     __shared__ int doff[8];
+    __shared__ __align__(8) uint64_t s_bar;
     const int g = blockIdx.y;
     const brp_params& P = a.params[g];
     const uint32_t window = P.window, fundamental = P.fundamental, harmonic = P.harmonic;
@@ -265,35 +267,60 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     const int64_t first = int64_t(blockIdx.x) * kHBlocks - 1;
     const int m = threadIdx.x;
 
-    // ---- stage the odd factors: 16-byte asynchronous copies from a 16-byte
-    // aligned start; chunks reaching outside [0, M) are copied element-wise
-    // with zero fill.
-    const uint32_t stage_sh = uint32_t(__cvta_generic_to_shared(stage));
-#pragma unroll 1
-    for (int k = 1; k <= 15; k += 2) {
-        const int64_t gs = first * k;
-        const int64_t ga = gs >= 0 ? (gs & ~int64_t(3)) : -((-gs + 3) & ~int64_t(3));
-        if (threadIdx.x == 0) doff[k / 2] = int(gs - ga);
-        const int chunks = region_floats(k) / 4;
-        const uint32_t reg = stage_sh + 4u * uint32_t(odd_base(k));
-        for (int c = threadIdx.x; c < chunks; c += kHThreads) {
-            const int64_t gi = ga + 4 * c;
-            const uint32_t dst = reg + 16u * uint32_t(c);
-            if (gi >= 0 && gi + 4 <= int64_t(M)) {
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(Pw + gi) : "memory");
-            } else {
+    // ---- stage the odd factors.  Interior CTAs (every region inside [0, M)):
+    // one bulk copy per region, issued by thread 0 and counted on an mbarrier.
+    // Edge CTAs: 16-byte asynchronous copies from a 16-byte aligned start,
+    // chunks reaching outside [0, M) copied element-wise with zero fill.
+    const uint32_t stage_sh = smem_u32(stage);
+    const uint32_t bar = smem_u32(&s_bar);
+    const bool bulk = first >= 0 && ((first * 15) & ~int64_t(3)) + region_floats(15) <= int64_t(M);
+    bool copied = true;
+    if (bulk) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            mbar_arrive_expect_tx(bar, uint32_t(kStageFloats) * 4u);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const bool in = gi + q >= 0 && gi + q < int64_t(M);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst + 4u * q),
-                                 "l"(Pw + (in ? gi + q : 0)), "r"(in ? 4 : 0)
-                                 : "memory");
+            for (int k = 1; k <= 15; k += 2) {
+                const int64_t gs = first * k, ga = gs & ~int64_t(3);
+                doff[k / 2] = int(gs - ga);
+                bulk_copy_g2s(stage_sh + 4u * uint32_t(odd_base(k)), Pw + ga, 4u * uint32_t(region_floats(k)), bar);
+            }
+        }
+        __syncthreads();  // the barrier is initialised before anyone polls it
+        copied = mbar_wait_bounded(bar, 0);
+    } else {
+#pragma unroll 1
+        for (int k = 1; k <= 15; k += 2) {
+            const int64_t gs = first * k;
+            const int64_t ga = gs >= 0 ? (gs & ~int64_t(3)) : -((-gs + 3) & ~int64_t(3));
+            if (threadIdx.x == 0) doff[k / 2] = int(gs - ga);
+            const int chunks = region_floats(k) / 4;
+            const uint32_t reg = stage_sh + 4u * uint32_t(odd_base(k));
+            for (int c = threadIdx.x; c < chunks; c += kHThreads) {
+                const int64_t gi = ga + 4 * c;
+                const uint32_t dst = reg + 16u * uint32_t(c);
+                if (gi >= 0 && gi + 4 <= int64_t(M)) {
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(Pw + gi) : "memory");
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const bool in = gi + q >= 0 && gi + q < int64_t(M);
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst + 4u * q),
+                                     "l"(Pw + (in ? gi + q : 0)), "r"(in ? 4 : 0)
+                                     : "memory");
+                    }
                 }
             }
         }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
     }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
+    if (__syncthreads_or(!copied)) {
+        // A bulk copy did not complete within the bound: report it, give the
+        // copies one more bounded wait (they write this CTA's shared memory) and leave.
+        if (threadIdx.x == 0) atomicOr(a.status + g, BRP_STATUS_WAIT_TIMEOUT);
+        mbar_wait_bounded(bar, 0);
+        return;
+    }
 
     HCtx c;
     c.stage = stage; c.doff = doff; c.Pw = Pw; c.m = m; c.M = M;

@@ -32,10 +32,11 @@ extern "C" {
 enum { BRP_OK = 0, BRP_E_RUNTIME = 1, BRP_E_RESULT = 2, BRP_E_TIMEOUT = 3, BRP_E_ARGUMENT = 4 };
 
 /* Per-template device error word bits (shaders/resample.comp:18,
- * shaders/harmonic.comp:34).  BRP_STATUS_MMA_TIMEOUT has no reference
- * counterpart: the tensor-core pass-1 form (compiled pass-1 configurations
- * 111-114) gave up waiting for its matrix multiplies. */
-enum { BRP_STATUS_OVERFLOW = 1u, BRP_STATUS_RESAMPLE_OOB = 2u, BRP_STATUS_MMA_TIMEOUT = 4u };
+ * shaders/harmonic.comp:34).  BRP_STATUS_WAIT_TIMEOUT has no reference
+ * counterpart: a kernel gave up a bounded wait for its own asynchronous work
+ * (the bulk copies that stage the harmonic kernel's power values, the matrix
+ * multiplies of the tensor-core pass-1 form, configurations 111-114). */
+enum { BRP_STATUS_OVERFLOW = 1u, BRP_STATUS_RESAMPLE_OOB = 2u, BRP_STATUS_WAIT_TIMEOUT = 4u };
 
 /* Byte-identical to brp::Params (include/brp/science.hpp:8-17, 108 bytes). */
 typedef struct brp_params {
