@@ -21,6 +21,7 @@ Reported (one JSON line, rank 0):
 select) with scipy's float32 real FFT standing in for FFTW, over all host cores.
 """
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -51,7 +52,7 @@ ALGO_BYTES = {"pass1": 8, "pass2": 6, "harmonic": 2}
 def parse():
     a = argparse.ArgumentParser()
     a.add_argument("--gpus", type=int, default=1)
-    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--steps", type=int, default=40)
     a.add_argument("--warmup", type=int, default=3)
     a.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     a.add_argument("--templates", type=int, default=TEMPLATES)
@@ -150,37 +151,60 @@ def reference_kind():
 
 # ------------------------------------------------------------------- clocks
 class Clocks:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    """nvidia-smi samples every 100 ms; only the samples whose timestamps fall
+    inside the timed region (begin() .. end()) are summarised."""
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index):
         self.proc = None
+        self.t0 = self.t1 = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device_index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)  # the sampler's start-up, before the timed region
         except Exception:
             self.proc = None
+
+    def begin(self):
+        self.t0 = datetime.datetime.now()
+
+    def end(self):
+        self.t1 = datetime.datetime.now()
 
     def stop(self):
         if not self.proc:
             return None
+        time.sleep(0.2)
         self.proc.terminate()
         try:
             out, _ = self.proc.communicate(timeout=5)
         except Exception:
             self.proc.kill()
             return None
-        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 7]
-        if not rows:
+        rows = []
+        for line in out.strip().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            if len(r) < 9:
+                continue
+            try:
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(r[1]), float(r[2]), r[5:9]))
+            except ValueError:
+                continue
+        inside = [r for r in rows if self.t0 and self.t1 and self.t0 <= r[0] <= self.t1]
+        use = inside or rows
+        if not use:
             return None
-        sm = [float(r[0]) for r in rows]
-        mx = max(float(r[1]) for r in rows)
+        sm = [r[1] for r in use]
+        mx = max(r[2] for r in use)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip().lower() == "active"})
+        reasons = sorted({names[i] for r in use for i in range(4) if r[3][i].lower() == "active"})
         loaded = [s for s in sm if s > 0.5 * mx] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(use),
+                "window": "timed region" if inside else "whole run (no sample inside the timed region)"}
 
 
 # --------------------------------------------------------------- reference arm
@@ -277,6 +301,7 @@ def main():
     # --- device throughput (value)
     clocks = Clocks(local)
     barrier()
+    clocks.begin()
     step_ms = []
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
@@ -289,6 +314,7 @@ def main():
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
     barrier()
+    clocks.end()
     clock = clocks.stop()
     dev_ms = sum(step_ms)
 
