@@ -421,11 +421,13 @@ struct brp_bank {
     brp_candidate* d_cands = nullptr;
     brp_candidate* d_compact = nullptr;
     uint64_t* d_offsets = nullptr;
+    uint32_t* d_rank = nullptr;  // per result slot: the caller's index of its template
     uint64_t compact_cap = 0;
     brp_params* h_params = nullptr;
     const float** h_inputs = nullptr;
     uint32_t* h_counts = nullptr;
     uint64_t* h_offsets = nullptr;
+    uint32_t* h_rank = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<uint64_t> graph_key;
@@ -466,6 +468,7 @@ struct brp_bank {
         if (h_inputs) cudaFreeHost(h_inputs);
         if (h_counts) cudaFreeHost(h_counts);
         if (h_offsets) cudaFreeHost(h_offsets);
+        if (h_rank) cudaFreeHost(h_rank);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -533,12 +536,15 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
         (st = b->alloc(&b->d_mean, max_templates, "mean")) ||
         (st = b->alloc(&b->d_cands, size_t(max_templates) * capacity, "candidates")) ||
         (st = b->alloc(&b->d_compact, b->compact_cap, "compact")) ||
-        (st = b->alloc(&b->d_offsets, size_t(max_templates) + 1, "offsets")))
+        (st = b->alloc(&b->d_offsets, size_t(max_templates) + 1, "offsets")) ||
+        (st = b->alloc(&b->d_rank, max_templates, "rank")) ||
+        (st = b->cuda(set_bank_compact_attributes(capacity), "compaction shared memory")))
         return cleanup(st);
     if ((st = b->cuda(cudaMallocHost(&b->h_params, max_templates * sizeof(brp_params)), "cudaMallocHost")) ||
         (st = b->cuda(cudaMallocHost(&b->h_inputs, max_templates * sizeof(void*)), "cudaMallocHost")) ||
         (st = b->cuda(cudaMallocHost(&b->h_counts, 2 * max_templates * sizeof(uint32_t)), "cudaMallocHost")) ||
-        (st = b->cuda(cudaMallocHost(&b->h_offsets, (max_templates + 1) * sizeof(uint64_t)), "cudaMallocHost")))
+        (st = b->cuda(cudaMallocHost(&b->h_offsets, (max_templates + 1) * sizeof(uint64_t)), "cudaMallocHost")) ||
+        (st = b->cuda(cudaMallocHost(&b->h_rank, max_templates * sizeof(uint32_t)), "cudaMallocHost")))
         return cleanup(st);
     *out = b;
     return BRP_OK;
@@ -627,7 +633,8 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         cudaStreamWaitEvent(s, b->join, 0);
     }
     mark(3, true);
-    launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_compact, b->compact_cap, b->d_offsets, s);
+    launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_rank, b->d_compact, b->compact_cap,
+                        b->d_offsets, s);
     mark(3, false);
     b->kernels_per_run = kernels + 1;
 }
@@ -656,6 +663,7 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     key.push_back(count);
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t t = order[k];
+        b->h_rank[k] = t;
         b->h_params[k] = templates[t];
         b->h_params[k].capacity = b->capacity;
         b->h_inputs[k] = b->d_series[series_of[t]];
@@ -667,7 +675,9 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     if ((st = b->cuda(cudaMemcpyAsync(b->d_params, b->h_params, count * sizeof(brp_params), cudaMemcpyHostToDevice, s),
                       "params upload")) ||
         (st = b->cuda(cudaMemcpyAsync(b->d_inputs, b->h_inputs, count * sizeof(void*), cudaMemcpyHostToDevice, s),
-                      "inputs upload")))
+                      "inputs upload")) ||
+        (st = b->cuda(cudaMemcpyAsync(b->d_rank, b->h_rank, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+                      "rank upload")))
         return st;
     b->last_sorted_n = sorted_n;
     b->last_spans = spans;
@@ -692,32 +702,23 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
     if (timed_out) return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
     if ((st = b->cuda(e, "bank search"))) return st;
+    // The compaction wrote the lists in the caller's order, each sorted by
+    // (level, bin); offsets are by caller index.
     const uint64_t total = b->h_offsets[count];
-    std::vector<brp_candidate> compact(total);
-    if (total && (st = b->cuda(cudaMemcpy(compact.data(), b->d_compact, total * sizeof(brp_candidate),
-                                          cudaMemcpyDeviceToHost), "candidates download")))
+    if (out && total && (st = b->cuda(cudaMemcpy(out, b->d_compact, std::min<uint64_t>(total, out_cap) *
+                                                 sizeof(brp_candidate), cudaMemcpyDeviceToHost),
+                                      "candidates download")))
         return st;
-    // Back to the caller's order, candidates sorted by (level, bin) per template.
-    std::vector<uint64_t> dst_off(count + 1, 0);
-    std::vector<uint32_t> kept(count);
+    bool bad = false;
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t t = order[k];
         counts[t] = b->h_counts[k];
         status[t] = h_status[k] | (b->h_counts[k] > b->capacity ? BRP_STATUS_OVERFLOW : 0u);
-        kept[t] = uint32_t(b->h_offsets[k + 1] - b->h_offsets[k]);
-    }
-    for (uint32_t t = 0; t < count; ++t) dst_off[t + 1] = dst_off[t] + kept[t];
-    bool bad = false;
-    for (uint32_t k = 0; k < count; ++k) {
-        const uint32_t t = order[k];
         if (status[t]) bad = true;
-        if (dst_off[t] + kept[t] > out_cap) { bad = true; continue; }
-        if (out) {
-            std::memcpy(out + dst_off[t], compact.data() + b->h_offsets[k], size_t(kept[t]) * sizeof(brp_candidate));
-            sort_candidates(out + dst_off[t], kept[t]);
-        }
+        const uint64_t first = b->h_offsets[t], kept = std::min(b->h_counts[k], b->capacity);
+        if (out && kept > kCompactSortMax && first + kept <= out_cap) sort_candidates(out + first, kept);
     }
-    if (dst_off[count] > out_cap) return b->fail(BRP_E_RESULT, "candidate output buffer too small");
+    if (total > out_cap) return b->fail(BRP_E_RESULT, "candidate output buffer too small");
     if (bad) return b->fail(BRP_E_RESULT, "GPU invalid resample index or candidate overflow; no valid result");
     return BRP_OK;
 }

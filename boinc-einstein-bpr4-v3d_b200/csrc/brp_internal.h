@@ -141,7 +141,13 @@ struct PlainArgs {
 // Records the plain pipeline on stream s; ev (optional, 5 events) brackets the 4 stages.
 void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev);
 
+// Candidate compaction of a bank run (plain_kernels.cu): slot k's list goes,
+// sorted by (level, bin), to the caller's position rank[k]; lists longer than
+// kCompactSortMax are copied unsorted (the host sorts them).
+constexpr uint32_t kCompactSortMax = 16384;
+cudaError_t set_bank_compact_attributes(uint32_t capacity);
 void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
-                         brp_candidate* out, uint64_t out_cap, uint64_t* offsets, cudaStream_t s);
+                         const uint32_t* rank, brp_candidate* out, uint64_t out_cap, uint64_t* offsets,
+                         cudaStream_t s);
 
 }  // namespace brp

@@ -163,6 +163,35 @@ static int by_significance(const void* x, const void* y) {
     return a->significance < b->significance ? 1 : (a->significance > b->significance ? -1 : 0);
 }
 
+// Re-sorts a level's 100 rows after row i was replaced by a row of higher
+// power (the reference calls qsort with by_power here).  The rows were sorted
+// before, so moving row i up to its place gives a sorted array; when no two
+// filled rows of the result have equal power (unfilled rows are all-zero and
+// interchangeable), that sorted order is the only one, so it is exactly what
+// qsort produces.  With a tie the order of equal rows is qsort's to decide, and
+// qsort is called as in the reference.
+static void resort_level(brp_bank_candidate* r, int i) {
+    const brp_bank_candidate row = r[i];
+    int j = i;
+    while (j > 0 && r[j - 1].power < row.power) --j;
+    // Equal powers among filled rows of the result: pairs already adjacent
+    // (those without row i), the pair that closes up where row i leaves (when
+    // it moves), and the moved row with its new upper neighbour.  Its new lower
+    // neighbour has lower power (it was below row i's old or new place).
+    bool tie = j > 0 && r[j - 1].power == row.power;
+    for (int m = 0; m + 1 < 100 && !tie; ++m)
+        if (m != i && m + 1 != i && r[m].harmonics && r[m + 1].harmonics && r[m].power == r[m + 1].power) tie = true;
+    if (!tie && j < i && i + 1 < 100 && i > 0 && r[i - 1].harmonics && r[i + 1].harmonics &&
+        r[i - 1].power == r[i + 1].power)
+        tie = true;
+    if (tie) {
+        std::qsort(r, 100, sizeof(brp_bank_candidate), by_power);
+        return;
+    }
+    std::memmove(r + j + 1, r + j, size_t(i - j) * sizeof(brp_bank_candidate));
+    r[j] = row;
+}
+
 extern "C" int brp_toplist_retain(brp_toplist* t, const brp_candidate* cands, uint32_t count, double period,
                                   double tau, double psi, const brp_params* p) {
     for (uint32_t k = 0; k < count; ++k) {
@@ -176,7 +205,7 @@ extern "C" int brp_toplist_retain(brp_toplist* t, const brp_candidate* cands, ui
             if (t->rows[i].bin == c.bin) { place = t->rows[i].power < c.power ? int(i) : -1; break; }
         if (place >= int(first)) {
             t->rows[place] = {c.power, float(period), float(tau), float(psi), 0, 1u << c.level, c.bin};
-            std::qsort(t->rows + first, 100, sizeof(brp_bank_candidate), by_power);
+            resort_level(t->rows + first, place - int(first));
         }
     }
     return BRP_OK;

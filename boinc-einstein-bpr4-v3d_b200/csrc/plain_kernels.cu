@@ -218,20 +218,33 @@ void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[4], s);
 }
 
-// Gathers the candidates of `count` result slots back to back:
-// offsets[t] = sum of min(counts[u], capacity) for u < t, offsets[count] = total.
-// One CTA per slot: it sums the clamped counts before its slot (a CTA-wide
-// reduction; count is at most a few thousand) and copies its slot's
-// candidates, 16 bytes per thread.
-static_assert(sizeof(brp_candidate) == 16, "candidates move as 16-byte vectors");
+// Gathers the candidates of `count` result slots back to back in the caller's
+// order, each slot's list sorted by (level, bin) -- the order the single-template
+// read-out gives (src/vulkan.cpp:329-337 returns a slot's list; the lists here
+// are sorted so that the result does not depend on the device's emission order).
+// Slot k holds the caller's template rank[k]; offsets[t] = sum of
+// min(counts[u], capacity) over the slots u with rank[u] < t, offsets[count] = total.
+// One CTA per slot: it sums the clamped counts of the slots before its
+// template, loads its list as 64-bit keys (level, bin, power bits; (level, bin)
+// is unique within a slot, so the sorted order is unique), sorts them in shared
+// memory (bitonic, padded to a power of two) and writes them out.  A list longer
+// than the shared-memory sort (kCompactSortMax) is copied unsorted and sorted by
+// the host.
+__host__ __device__ constexpr uint32_t compact_sort_size(uint32_t capacity) {
+    uint32_t p = 2;
+    while (p < capacity && p < kCompactSortMax) p <<= 1;
+    return p;
+}
 
 __global__ void __launch_bounds__(256) bank_compact_kernel(const uint32_t* counts, const brp_candidate* cands,
-                                                           uint32_t capacity, uint32_t count, brp_candidate* out,
-                                                           uint64_t out_cap, uint64_t* offsets) {
+                                                           uint32_t capacity, uint32_t count, const uint32_t* rank,
+                                                           brp_candidate* out, uint64_t out_cap, uint64_t* offsets) {
+    extern __shared__ unsigned long long keys[];
     __shared__ uint64_t s_part[8];
-    const uint32_t t = blockIdx.x;
+    const uint32_t k = blockIdx.x, t = rank[k];
     uint64_t acc = 0;
-    for (uint32_t u = threadIdx.x; u < t; u += blockDim.x) acc += min(counts[u], capacity);
+    for (uint32_t u = threadIdx.x; u < count; u += blockDim.x)
+        if (rank[u] < t) acc += min(counts[u], capacity);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
@@ -239,20 +252,62 @@ __global__ void __launch_bounds__(256) bank_compact_kernel(const uint32_t* count
     uint64_t off = 0;
 #pragma unroll
     for (int w = 0; w < 8; ++w) off += s_part[w];
-    const uint32_t c = min(counts[t], capacity);
+    const uint32_t c = min(counts[k], capacity);
     if (threadIdx.x == 0) {
         offsets[t] = off;
         if (t + 1 == count) offsets[count] = off + c;
     }
-    const uint4* src = reinterpret_cast<const uint4*>(cands + size_t(t) * capacity);
-    uint4* dst = reinterpret_cast<uint4*>(out);
-    for (uint32_t k = threadIdx.x; k < c; k += blockDim.x)
-        if (off + k < out_cap) dst[off + k] = src[k];
+    const brp_candidate* src = cands + size_t(k) * capacity;
+    if (c > kCompactSortMax) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(out);
+        for (uint32_t i = threadIdx.x; i < c; i += blockDim.x)
+            if (off + i < out_cap) d4[off + i] = s4[i];
+        return;
+    }
+    uint32_t P = 2;
+    while (P < c) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+        unsigned long long key = ~0ull;
+        if (i < c) {
+            const brp_candidate x = src[i];
+            key = (static_cast<unsigned long long>(x.level) << 55) | (static_cast<unsigned long long>(x.bin) << 32) |
+                  __float_as_uint(x.power);
+        }
+        keys[i] = key;
+    }
+    __syncthreads();
+    for (uint32_t w = 2; w <= P; w <<= 1) {
+        for (uint32_t j = w >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P / 2; i += blockDim.x) {
+                const uint32_t lo = ((i & ~(j - 1)) << 1) | (i & (j - 1)), hi = lo | j;
+                const unsigned long long x = keys[lo], y = keys[hi];
+                if ((x > y) == ((lo & w) == 0)) { keys[lo] = y; keys[hi] = x; }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+        if (off + i >= out_cap) break;
+        const unsigned long long key = keys[i];
+        brp_candidate x;
+        x.level = uint32_t(key >> 55); x.bin = uint32_t(key >> 32) & 0x7FFFFFu; x.power = __uint_as_float(uint32_t(key));
+        x.reserved = 0;
+        out[off + i] = x;
+    }
+}
+
+cudaError_t set_bank_compact_attributes(uint32_t capacity) {
+    return cudaFuncSetAttribute(bank_compact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(compact_sort_size(capacity) * sizeof(unsigned long long)));
 }
 
 void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
-                         brp_candidate* out, uint64_t out_cap, uint64_t* offsets, cudaStream_t s) {
-    if (count) bank_compact_kernel<<<count, 256, 0, s>>>(counts, cands, capacity, count, out, out_cap, offsets);
+                         const uint32_t* rank, brp_candidate* out, uint64_t out_cap, uint64_t* offsets,
+                         cudaStream_t s) {
+    if (count)
+        bank_compact_kernel<<<count, 256, compact_sort_size(capacity) * sizeof(unsigned long long), s>>>(
+            counts, cands, capacity, count, rank, out, out_cap, offsets);
 }
 
 }  // namespace brp

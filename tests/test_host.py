@@ -126,3 +126,27 @@ def test_toplist_fold_equals_sequential_retain(oracle):
     for q, o, c in zip(temps, orbs, cands):
         ref.retain(c, *o, ref.thresholds(q))
     assert a.tobytes() == ref.final().tobytes() and len(a) > 0
+
+
+@pytest.mark.parametrize("quantum", [0.0, 0.5])
+def test_toplist_long_stream_with_and_without_ties(oracle, quantum):
+    """A long candidate stream (every template above the current row 100, as at
+    the start of a bank) through the product's toplist, the oracle's and the
+    reference's own code.  quantum > 0 rounds the powers so that many filled
+    rows tie (the qsort path); quantum 0 keeps them distinct (the insertion path)."""
+    rng = np.random.default_rng(13)
+    p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
+    tops = [B.Toplist(), oracle.Toplist()]
+    if oracle.ref_available():
+        tops.append(oracle.RefToplist())
+    for t in range(150):
+        c = _random_candidates(rng, p, 120)
+        if quantum:
+            c["power"] = np.round(c["power"] / quantum) * quantum
+        orb = (3600.0 + t, 0.01 * t, 0.1 * t)
+        for tl in tops:
+            tl.retain(c, *orb, tl.thresholds(p))
+    finals = [tl.final() for tl in tops]
+    for f in finals[1:]:
+        assert f.tobytes() == finals[0].tobytes()
+    assert len(finals[0]) > 0
