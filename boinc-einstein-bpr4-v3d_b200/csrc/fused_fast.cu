@@ -66,6 +66,78 @@ __device__ __forceinline__ uint32_t pass2_row(int rr, int R, uint32_t q, uint32_
     return ar == 0 ? L1 / 2 : L1 - ar;
 }
 
+// Real-spectrum post-process of one bin pair k (row arow = k mod L1, arow != 0)
+// and km = M - k: X_k and X_{M-k} from Z_k, Z_{M-k}, the padding term and the
+// normalised power.  wa = W_n^{k steps}.
+struct PostArgs {
+    const float2 *hf_hi, *hf_lo;
+    float* Pw;
+    float2* fft;
+    float inv_n, fn, hm;  // 1/n, n, -mean/2
+    bool pow2, a_odd;
+};
+
+__device__ __forceinline__ void post_pair(const PostArgs& c, uint32_t k, uint32_t km, float2 zk, float2 zm,
+                                          float2 wa) {
+    // cos, sin of pi k / n from the W_2n table; W_n^k = (cos - i sin)^2
+    const float2 hf = twiddle2(c.hf_hi, c.hf_lo, kSplitLog2, k);
+    const float cv = hf.x, sv = -hf.y;
+    const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
+    const float2 wm = make_float2(-w.x, w.y);
+    const float2 wam = c.a_odd ? make_float2(-wa.x, wa.y) : make_float2(wa.x, -wa.y);
+    const float2 G1 = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
+    const float2 G2 = cmul(make_float2(1.f - wam.x, -wam.y), make_float2(cv, -sv));
+    const float f1 = __fdividef(c.hm, sv), f2 = __fdividef(c.hm, cv);
+    const float2 X1 = real_bin(zk, zm, w, make_float2(G1.x * f1, G1.y * f1));
+    const float2 X2 = real_bin(zm, zk, wm, make_float2(G2.x * f2, G2.y * f2));
+    const float p1 = X1.x * X1.x + X1.y * X1.y, p2 = X2.x * X2.x + X2.y * X2.y;
+    c.Pw[k] = c.pow2 ? p1 * c.inv_n : p1 / c.fn;
+    c.Pw[km] = c.pow2 ? p2 * c.inv_n : p2 / c.fn;
+    if (c.fft) { c.fft[k] = X1; c.fft[km] = X2; }
+}
+
+// Pass 2 of a CTA without row 0 (q > 0): the row passes but the last in shared
+// memory, then the last pass (span Ns, radix RL, Ns RL = L2) fused with the
+// post-process.  Thread t takes row pair r = t % R and butterfly j = t / R of
+// row r together with butterfly Ns - 1 - j of the mirror row: output m of the
+// first is Z at k2 = j + Ns m, output RL - 1 - m of the second Z of the mirror
+// row at L2 - 1 - k2, exactly the pair the post-process needs.
+template <int L2, int STRIDE, int R, int THREADS, int Ns, int RL, int... Rest>
+__device__ __forceinline__ void pass2_pairs(float2* sm, const float2* __restrict__ tw, const PostArgs& pc,
+                                            const float2* rl_hi, const float2* rl_lo, uint32_t q, uint32_t L1,
+                                            uint32_t n, uint32_t steps) {
+    if constexpr (sizeof...(Rest) > 0) {
+        ct_pass<L2, STRIDE, 2 * R, THREADS, Ns, RL>(sm, tw);
+        pass2_pairs<L2, STRIDE, R, THREADS, Ns * RL, Rest...>(sm, tw + (Ns > 1 ? Ns * TwStride<RL>::value : 0), pc,
+                                                            rl_hi, rl_lo, q, L1, n, steps);
+    } else {
+        static_assert(Ns * RL == L2 && R * Ns == THREADS, "one bin-pair butterfly pair per thread");
+        constexpr int NBF = L2 / RL;
+        const int r = threadIdx.x % R, j = threadIdx.x / R, jm = Ns - 1 - j;
+        float2 v[RL], u[RL];
+#pragma unroll
+        for (int i = 0; i < RL; ++i) {
+            v[i] = sm[r * STRIDE + ct_pos(j + i * NBF)];
+            u[i] = sm[(R + r) * STRIDE + ct_pos(jm + i * NBF)];
+        }
+        ct_twiddle<RL, Ns>(v, tw, j);
+        ct_twiddle<RL, Ns>(u, tw, jm);
+        dft<RL>(v);
+        dft<RL>(u);
+        const uint32_t arow = q * R + r, brow = L1 - arow;
+        const float2 wa_step = twiddle2(rl_hi, rl_lo, kSplitLog2, mod_n(uint64_t(L1) * Ns * steps, n));
+        float2 wa;
+#pragma unroll
+        for (int m = 0; m < RL; ++m) {
+            const uint32_t k2 = uint32_t(j + Ns * m);
+            const uint32_t k = arow + L1 * k2, km = brow + L1 * (uint32_t(L2) - 1 - k2);
+            if (m % 4 == 0) wa = twiddle2(rl_hi, rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
+            else wa = cmul(wa, wa_step);
+            post_pair(pc, k, km, v[m], u[RL - 1 - m], wa);
+        }
+    }
+}
+
 template <int L2, int R, int THREADS, int MINB, int R0, int... Rest>
 __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     constexpr int SEQ = 2 * R, STRIDE = ct_stride(L2, R);
@@ -112,15 +184,26 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     __syncthreads();
     const float mean = s_mean;
 
-    if constexpr (FIRST) ct_fft<L2, STRIDE, SEQ, THREADS, 16, Rest...>(sm, a.ptw2);
-    else ct_fft<L2, STRIDE, SEQ, THREADS, 1, R0, Rest...>(sm, a.ptw2);
-
     float* __restrict__ Pw = a.power + size_t(g) * a.power_stride;
     float2* fft = (g == a.snap) ? a.snap_fft : nullptr;
     const bool pow2 = (n & (n - 1)) == 0;
     const float inv_n = 1.0f / float(n), fn = float(n);
     const bool a_odd = steps & 1u;
     const float pad0 = float(n - steps) * mean;
+    PostArgs pc;
+    pc.hf_hi = a.hf_hi; pc.hf_lo = a.hf_lo; pc.Pw = Pw; pc.fft = fft;
+    pc.inv_n = inv_n; pc.fn = fn; pc.hm = -0.5f * mean; pc.pow2 = pow2; pc.a_odd = a_odd;
+
+    if (q > 0) {
+        if constexpr (FIRST)
+            pass2_pairs<L2, STRIDE, R, THREADS, 16, Rest...>(sm, a.ptw2, pc, a.rl_hi, a.rl_lo, q, L1, n, steps);
+        else
+            pass2_pairs<L2, STRIDE, R, THREADS, 1, R0, Rest...>(sm, a.ptw2, pc, a.rl_hi, a.rl_lo, q, L1, n, steps);
+        return;
+    }
+    // CTA 0 (row 0 and row L1/2 pair with themselves): all passes in shared memory.
+    if constexpr (FIRST) ct_fft<L2, STRIDE, SEQ, THREADS, 16, Rest...>(sm, a.ptw2);
+    else ct_fft<L2, STRIDE, SEQ, THREADS, 1, R0, Rest...>(sm, a.ptw2);
 
     // Thread t keeps row pair r = t % R and visits k2 = t / R + it THREADS / R,
     // so k = qR + r + L1 k2 advances by L1 THREADS / R: W_n^{k steps} comes from
@@ -165,24 +248,9 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             const uint32_t k = arow + L1 * k2;
             const uint32_t km = brow + L1 * uint32_t(L2 - 1 - k2);
             const float2 zk = sm[r * STRIDE + ct_pos(k2)], zm = sm[(R + r) * STRIDE + ct_pos(L2 - 1 - k2)];
-            // cos, sin of pi k / n from the W_2n table; W_n^k = (cos - i sin)^2
-            const float2 hf = twiddle2(a.hf_hi, a.hf_lo, kSplitLog2, k);
-            const float cv = hf.x, sv = -hf.y;
-            const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
             if (it % 4 == 0) wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
             else wa = cmul(wa, wa_step);
-            const float2 wm = make_float2(-w.x, w.y);
-            const float2 wam = a_odd ? make_float2(-wa.x, wa.y) : make_float2(wa.x, -wa.y);
-            const float2 G1 = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
-            const float2 G2 = cmul(make_float2(1.f - wam.x, -wam.y), make_float2(cv, -sv));
-            const float hm = -0.5f * mean;
-            const float f1 = __fdividef(hm, sv), f2 = __fdividef(hm, cv);
-            const float2 X1 = real_bin(zk, zm, w, make_float2(G1.x * f1, G1.y * f1));
-            const float2 X2 = real_bin(zm, zk, wm, make_float2(G2.x * f2, G2.y * f2));
-            const float p1 = X1.x * X1.x + X1.y * X1.y, p2 = X2.x * X2.x + X2.y * X2.y;
-            Pw[k] = pow2 ? p1 * inv_n : p1 / fn;
-            Pw[km] = pow2 ? p2 * inv_n : p2 / fn;
-            if (fft) { fft[k] = X1; fft[km] = X2; }
+            post_pair(pc, k, km, zk, zm, wa);
         }
     }
 }
