@@ -59,6 +59,8 @@ def parse():
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-plain", action="store_true")
     a.add_argument("--no-tune", action="store_true", help="skip the autotuner (default kernels)")
+    a.add_argument("--plan", default=None,
+                   help="pass1,pass2,group,chains: use this configuration instead of the autotuner")
     return a.parse_args()
 
 
@@ -281,7 +283,11 @@ def main():
     # autotune the kernel configuration and templates per launch on this bank
     # (untimed), then warm up through the public API (captures the graph)
     plan = None
-    if not args.no_tune:
+    if args.plan:
+        p1, p2, grp, ch = (int(v) for v in args.plan.split(","))
+        bank.configure(N, pass1=p1, pass2=p2, group=grp, chains=ch)
+        plan = {str(N): {"pass1": p1, "pass2": p2, "group": grp, "chains": ch, "ms": None}}
+    elif not args.no_tune:
         from brp_b200 import tune
         bank.set_series(0, x_host)
         res = tune.autotune(bank, my_templates, use_cache=False)
