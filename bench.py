@@ -61,6 +61,9 @@ def parse():
     a.add_argument("--no-tune", action="store_true", help="skip the autotuner (default kernels)")
     a.add_argument("--plan", default=None,
                    help="pass1,pass2,group,chains: use this configuration instead of the autotuner")
+    a.add_argument("--workload", default="bank", choices=["bank", "mixed-radix", "uneven"],
+                   help="bank: N=2^22, 512 templates (the headline); mixed-radix: N=3*2^21, 128 templates; "
+                        "uneven: 1024 templates over N in {2^20, 3*2^20, 2^22} (1 GPU, documentation runs)")
     return a.parse_args()
 
 
@@ -243,6 +246,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "bank":
+        return run_other_workload(args)
 
     total_templates = args.templates * world
     wl = workload(total_templates)
@@ -408,6 +413,90 @@ def main():
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def run_other_workload(args):
+    """The mixed-radix and uneven banks on one GPU: device time of the captured
+    graph (L2 flushed between steps), end to end through the public API
+    (series H2D, graph, candidates D2H, toplist fold per length class in bank
+    order), algorithmic HBM bytes 16 n per template over all kernels."""
+    from brp_b200 import synth, tune
+    import torch
+    import brp_b200 as B
+    wl = synth.config4() if args.workload == "mixed-radix" else synth.config5()
+    count = len(wl.templates)
+    bank = B.Bank(wl.n, [len(x) for x in wl.series], count, CAPACITY)
+    hosts = [torch.from_numpy(x).pin_memory().numpy() for x in wl.series]
+    for s, x in enumerate(hosts):
+        bank.set_series(s, x)
+    if args.plan:  # single-length workloads: a fixed configuration (e.g. the tensor-core pass 1)
+        p1, p2, grp, ch = (int(v) for v in args.plan.split(","))
+        bank.configure(wl.n[0], pass1=p1, pass2=p2, group=grp, chains=ch)
+        plan = {str(wl.n[0]): {"pass1": p1, "pass2": p2, "group": grp, "chains": ch, "ms": None}}
+    else:
+        res = tune.autotune(bank, wl.templates, wl.series_of, use_cache=False)
+        plan = {str(n): {k: r[k] for k in ("pass1", "pass2", "group", "chains", "ms")} for n, r in res.items()}
+    tarr = B.Bank.params_array(wl.templates)
+    so = np.asarray(wl.series_of, np.uint32)
+    orbits = np.asarray(wl.orbits, np.float64)
+    out = np.empty(count * CAPACITY, B.CANDIDATE)
+    classes = sorted(set(int(v) for v in wl.series_of))
+    members = {s: np.flatnonzero(so == s) for s in classes}
+    class_params = {s: B.Bank.params_array([wl.templates[t] for t in members[s]]) for s in classes}
+
+    def e2e_step():
+        for s, x in enumerate(hosts):
+            bank.set_series(s, x)
+        flat, offs, counts, status = bank.run_flat(tarr, so, out=out)
+        tops = {}
+        for s in classes:  # one toplist per series, its templates in bank order
+            idx = members[s]
+            if len(idx) and idx[-1] - idx[0] + 1 == len(idx):  # contiguous in the bank
+                cand = flat[offs[idx[0]]:offs[idx[-1] + 1]]
+            else:
+                cand = np.concatenate([flat[offs[t]:offs[t + 1]] for t in idx]) if len(idx) else flat[:0]
+            tops[s] = B.Toplist().fold(class_params[s], orbits[idx], cand, counts[idx])
+        return tops
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    stream = torch.cuda.ExternalStream(bank.stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.begin()
+    step_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bank.launch()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    clocks.end()
+    clock = clocks.stop()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = 1000 * (time.perf_counter() - t0)
+    kernel_ms, launches = bank.profile()
+    dev_ms = sum(step_ms)
+    algo = sum(16 * wl.n[s] for s in wl.series_of)
+    print(json.dumps({
+        "metric": "orbital templates/s (%s bank on 1 B200)" % args.workload, "value": count * args.steps / (dev_ms / 1e3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "lengths": list(wl.n),
+                   "templates_per_length": [int(len(members.get(s, []))) for s in range(len(wl.n))],
+                   "candidate_capacity": CAPACITY, "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
+                   "plan": plan},
+        "e2e": {"value": count * args.steps / (e2e_ms / 1e3), "unit": UNIT},
+        "algorithmic_hbm_gbs": algo / (dev_ms / args.steps * 1e-3) / 1e9,
+        "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": launches, "clocks": clock}), flush=True)
+    bank.close()
 
 
 def spectrum_error(B, wl, p):
