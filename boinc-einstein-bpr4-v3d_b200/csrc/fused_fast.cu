@@ -308,6 +308,8 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<1536, 4, 384, 2, 8, 8, 8, 3>::info(105),
         P1<3072, 2, 384, 2, 16, 16, 4, 3>::info(106),
         P1<512, 8, 256, 4, 8, 8, 8>::info(107),
+        P1<512, 8, 256, 4, 16, 8, 4>::info(108),
+        P1<1536, 4, 384, 2, 16, 8, 4, 3>::info(109),
     };
     append_pass1_tc_configs(v);
     return v;
