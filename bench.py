@@ -61,6 +61,8 @@ def parse():
     a.add_argument("--no-tune", action="store_true", help="skip the autotuner (default kernels)")
     a.add_argument("--plan", default=None,
                    help="pass1,pass2,group,chains: use this configuration instead of the autotuner")
+    a.add_argument("--toplist-rows", type=int, default=100,
+                   help="device toplist pre-filter rows per level (0: return every candidate)")
     a.add_argument("--workload", default="bank", choices=["bank", "mixed-radix", "uneven"],
                    help="bank: N=2^22, 512 templates (the headline); mixed-radix: N=3*2^21, 128 templates; "
                         "uneven: 1024 templates over N in {2^20, 3*2^20, 2^22} (1 GPU, documentation runs)")
@@ -299,9 +301,10 @@ def main():
         plan = {str(n): {k: r[k] for k in ("pass1", "pass2", "group", "chains", "ms")} for n, r in res.items()}
         if os.environ.get("BRP_BENCH_VERBOSE"):
             print(json.dumps({"tuning": {str(n): r.get("tried") for n, r in res.items()}}), file=sys.stderr)
+    bank.set_toplist_filter(args.toplist_rows)  # candidates that can reach the toplist
     for _ in range(max(args.warmup, 3)):
         flat, offs, counts, status = e2e_step()
-    d2h = 4 * count * 2 + 8 * (count + 1) + 16 * len(flat)
+    d2h = 4 * count * (3 if args.toplist_rows else 2) + 8 * (count + 1) + 16 * len(flat)
     h2d = 4 * N + 108 * count + 8 * count
 
     def barrier():
@@ -389,6 +392,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "bank search, N=2^22, %d templates per GPU, 3 injected pulsars" % args.templates,
                    "n": N, "templates_per_gpu": count, "candidate_capacity": CAPACITY,
+                   "toplist_prefilter_rows": args.toplist_rows,
                    "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
                    "parallelism": "template shards, %d rank(s)" % world,
                    "plan": plan},
@@ -458,6 +462,7 @@ def run_other_workload(args):
             tops[s] = B.Toplist().fold(class_params[s], orbits[idx], cand, counts[idx])
         return tops
 
+    bank.set_toplist_filter(args.toplist_rows)  # candidates that can reach the toplist
     for _ in range(max(args.warmup, 3)):
         e2e_step()
     stream = torch.cuda.ExternalStream(bank.stream)
@@ -491,7 +496,8 @@ def run_other_workload(args):
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": wl.name, "lengths": list(wl.n),
                    "templates_per_length": [int(len(members.get(s, []))) for s in range(len(wl.n))],
-                   "candidate_capacity": CAPACITY, "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
+                   "candidate_capacity": CAPACITY, "toplist_prefilter_rows": args.toplist_rows,
+                   "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
                    "plan": plan},
         "e2e": {"value": count * args.steps / (e2e_ms / 1e3), "unit": UNIT},
         "algorithmic_hbm_gbs": algo / (dev_ms / args.steps * 1e-3) / 1e9,

@@ -81,6 +81,11 @@ class Bank:
         parallel launch chains for length n."""
         check(lib().brp_cuda_bank_configure(self._b, n, pass1, pass2, group, chains), self._err)
 
+    def set_toplist_filter(self, rows=100):
+        """Return only the candidates that can reach a per-series toplist of
+        `rows` rows per level (0: all candidates); counts become the kept counts."""
+        check(lib().brp_cuda_bank_set_toplist_filter(self._b, rows), self._err)
+
     def launch(self):
         """Replays the last run's graph on the device only (no copies, no wait)."""
         check(lib().brp_cuda_bank_launch(self._b), self._err)

@@ -423,6 +423,10 @@ struct brp_bank {
     uint64_t* d_offsets = nullptr;
     uint32_t* d_rank = nullptr;  // per result slot: the caller's index of its template
     uint64_t compact_cap = 0;
+    // toplist pre-filter (off while filter_rows == 0)
+    uint32_t filter_rows = 0;
+    uint32_t *d_slot_series = nullptr, *h_slot_series = nullptr, *h_kept = nullptr;
+    FilterArgs filter{};
     brp_params* h_params = nullptr;
     const float** h_inputs = nullptr;
     uint32_t* h_counts = nullptr;
@@ -469,6 +473,8 @@ struct brp_bank {
         if (h_counts) cudaFreeHost(h_counts);
         if (h_offsets) cudaFreeHost(h_offsets);
         if (h_rank) cudaFreeHost(h_rank);
+        if (h_slot_series) cudaFreeHost(h_slot_series);
+        if (h_kept) cudaFreeHost(h_kept);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -633,8 +639,16 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         cudaStreamWaitEvent(s, b->join, 0);
     }
     mark(3, true);
+    const FilterArgs* filter = nullptr;
+    if (b->filter_rows) {
+        b->filter.counts = b->d_counts; b->filter.cands = b->d_cands; b->filter.capacity = b->capacity;
+        b->filter.count = count; b->filter.slot_series = b->d_slot_series;
+        launch_toplist_filter(b->filter, s);
+        filter = &b->filter;
+        kernels += 4;
+    }
     launch_bank_compact(b->d_counts, b->d_cands, b->capacity, count, b->d_rank, b->d_compact, b->compact_cap,
-                        b->d_offsets, s);
+                        b->d_offsets, filter, s);
     mark(3, false);
     b->kernels_per_run = kernels + 1;
 }
@@ -661,9 +675,11 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     std::vector<uint32_t> sorted_n(count), spans(count);
     std::vector<uint64_t> key;
     key.push_back(count);
+    key.push_back(b->filter_rows);
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t t = order[k];
         b->h_rank[k] = t;
+        if (b->h_slot_series) b->h_slot_series[k] = series_of[t];
         b->h_params[k] = templates[t];
         b->h_params[k].capacity = b->capacity;
         b->h_inputs[k] = b->d_series[series_of[t]];
@@ -677,7 +693,11 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
         (st = b->cuda(cudaMemcpyAsync(b->d_inputs, b->h_inputs, count * sizeof(void*), cudaMemcpyHostToDevice, s),
                       "inputs upload")) ||
         (st = b->cuda(cudaMemcpyAsync(b->d_rank, b->h_rank, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
-                      "rank upload")))
+                      "rank upload")) ||
+        (b->filter_rows &&
+         (st = b->cuda(cudaMemcpyAsync(b->d_slot_series, b->h_slot_series, count * sizeof(uint32_t),
+                                       cudaMemcpyHostToDevice, s),
+                       "slot series upload"))))
         return st;
     b->last_sorted_n = sorted_n;
     b->last_spans = spans;
@@ -697,6 +717,7 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     cudaMemcpyAsync(b->h_counts, b->d_counts, count * 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(h_status, b->d_status, count * 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(b->h_offsets, b->d_offsets, (count + 1) * 8, cudaMemcpyDeviceToHost, s);
+    if (b->filter_rows) cudaMemcpyAsync(b->h_kept, b->filter.kept, count * 4, cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b->done, s);
     bool timed_out = false;
     cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
@@ -712,10 +733,11 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     bool bad = false;
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t t = order[k];
-        counts[t] = b->h_counts[k];
+        const uint32_t kept = b->filter_rows ? b->h_kept[k] : std::min(b->h_counts[k], b->capacity);
+        counts[t] = b->filter_rows ? kept : b->h_counts[k];
         status[t] = h_status[k] | (b->h_counts[k] > b->capacity ? BRP_STATUS_OVERFLOW : 0u);
         if (status[t]) bad = true;
-        const uint64_t first = b->h_offsets[t], kept = std::min(b->h_counts[k], b->capacity);
+        const uint64_t first = b->h_offsets[t];
         if (out && kept > kCompactSortMax && first + kept <= out_cap) sort_candidates(out + first, kept);
     }
     if (total > out_cap) return b->fail(BRP_E_RESULT, "candidate output buffer too small");
@@ -756,6 +778,46 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
     cb.chains = ch;
     free_length_plan(it->second);
     it->second = lp;
+    b->graph_key.clear();
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_bank_set_toplist_filter(brp_bank* b, uint32_t rows) {
+    if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    if ((st = b->cuda(cudaStreamSynchronize(b->stream), "toplist filter"))) return st;
+    if (rows && !b->filter.maxkey) {
+        // Per series the per-bin arrays of its five levels, n/2 bins each.
+        const uint32_t S = uint32_t(b->n.size());
+        std::vector<uint64_t> base(S);
+        std::vector<uint32_t> half(S);
+        uint64_t total = 0;
+        for (uint32_t s = 0; s < S; ++s) { base[s] = total; half[s] = b->n[s] / 2; total += 5ull * half[s]; }
+        if (total >= (1ull << 32)) return b->fail(BRP_E_ARGUMENT, "toplist filter: series too long");
+        uint64_t* d_base = nullptr;
+        uint32_t* d_half = nullptr;
+        if ((st = b->alloc(&b->filter.maxkey, total, "filter")) || (st = b->alloc(&b->filter.flag, total, "filter")) ||
+            (st = b->alloc(&b->filter.owners, total, "filter")) ||
+            (st = b->alloc(&b->filter.owner_count, size_t(S) * 5, "filter")) ||
+            (st = b->alloc(&b->filter.threshold_key, size_t(S) * 5, "filter")) ||
+            (st = b->alloc(&b->filter.kept, b->max_templates, "filter")) ||
+            (st = b->alloc(&b->d_slot_series, b->max_templates, "filter")) || (st = b->alloc(&d_base, S, "filter")) ||
+            (st = b->alloc(&d_half, S, "filter")) ||
+            (st = b->cuda(cudaMemset(b->filter.maxkey, 0, total * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemset(b->filter.flag, 0, total * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemset(b->filter.owner_count, 0, size_t(S) * 5 * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemcpy(d_base, base.data(), S * 8, cudaMemcpyHostToDevice), "filter upload")) ||
+            (st = b->cuda(cudaMemcpy(d_half, half.data(), S * 4, cudaMemcpyHostToDevice), "filter upload")) ||
+            (st = b->cuda(cudaMallocHost(&b->h_slot_series, b->max_templates * sizeof(uint32_t)), "cudaMallocHost")) ||
+            (st = b->cuda(cudaMallocHost(&b->h_kept, b->max_templates * sizeof(uint32_t)), "cudaMallocHost")))
+            return st;
+        b->filter.base = d_base;
+        b->filter.half = d_half;
+        b->filter.series = S;
+    }
+    b->filter_rows = rows;
+    b->filter.rows = rows;
     b->graph_key.clear();
     return BRP_OK;
 }

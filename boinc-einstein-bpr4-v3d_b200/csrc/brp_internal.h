@@ -141,13 +141,47 @@ struct PlainArgs {
 // Records the plain pipeline on stream s; ev (optional, 5 events) brackets the 4 stages.
 void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev);
 
+// Device toplist pre-filter of a bank run (toplist_filter.cu).  Per series s
+// the per-bin arrays of level h start at base[s] + h * half[s] (half = n/2).
+struct FilterArgs {
+    const uint32_t* counts;       // per slot: candidate count (may exceed capacity)
+    const brp_candidate* cands;   // per slot: capacity candidates
+    uint32_t capacity, count;     // slots
+    const uint32_t* slot_series;  // per slot: series index
+    uint32_t series, rows;        // series count; toplist rows per level
+    const uint64_t* base;         // per series
+    const uint32_t* half;         // per series
+    uint32_t* maxkey;             // per (series, level, bin): highest power key
+    uint32_t* flag;               // per (series, level, bin)
+    uint32_t* owners;             // per (series, level): keys of the per-bin maxima
+    uint32_t* owner_count;        // per (series, level)
+    uint32_t* threshold_key;      // per (series, level): the rows-th largest per-bin maximum
+    uint32_t* kept;               // per slot: candidates that pass
+};
+void launch_toplist_filter(const FilterArgs& f, cudaStream_t s);
+
+#ifdef __CUDACC__
+// Order-preserving unsigned image of an FP32 power.
+__device__ __forceinline__ uint32_t power_key(float x) {
+    const uint32_t b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+// Whether candidate x of a slot of series s passes the filter (out-of-range
+// candidates pass, so that the host sees and rejects them).
+__device__ __forceinline__ bool filter_keep(const FilterArgs& f, uint32_t s, const brp_candidate& x) {
+    if (x.level >= 5 || x.bin >= f.half[s]) return true;
+    return power_key(x.power) >= f.threshold_key[s * 5 + x.level];
+}
+#endif
+
 // Candidate compaction of a bank run (plain_kernels.cu): slot k's list goes,
 // sorted by (level, bin), to the caller's position rank[k]; lists longer than
-// kCompactSortMax are copied unsorted (the host sorts them).
+// kCompactSortMax are copied unsorted (the host sorts them).  With `filter`
+// only the candidates that pass the toplist pre-filter are written.
 constexpr uint32_t kCompactSortMax = 16384;
 cudaError_t set_bank_compact_attributes(uint32_t capacity);
 void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
                          const uint32_t* rank, brp_candidate* out, uint64_t out_cap, uint64_t* offsets,
-                         cudaStream_t s);
+                         const FilterArgs* filter, cudaStream_t s);
 
 }  // namespace brp

@@ -229,52 +229,67 @@ void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
 // is unique within a slot, so the sorted order is unique), sorts them in shared
 // memory (bitonic, padded to a power of two) and writes them out.  A list longer
 // than the shared-memory sort (kCompactSortMax) is copied unsorted and sorted by
-// the host.
+// the host.  With the toplist pre-filter (toplist_filter.cu) a slot writes only
+// the candidates that pass it, and the offsets sum those kept counts.
 __host__ __device__ constexpr uint32_t compact_sort_size(uint32_t capacity) {
     uint32_t p = 2;
     while (p < capacity && p < kCompactSortMax) p <<= 1;
     return p;
 }
 
+__device__ __forceinline__ unsigned long long compact_key(const brp_candidate& x) {
+    return (static_cast<unsigned long long>(x.level) << 55) | (static_cast<unsigned long long>(x.bin) << 32) |
+           __float_as_uint(x.power);
+}
+
 __global__ void __launch_bounds__(256) bank_compact_kernel(const uint32_t* counts, const brp_candidate* cands,
                                                            uint32_t capacity, uint32_t count, const uint32_t* rank,
-                                                           brp_candidate* out, uint64_t out_cap, uint64_t* offsets) {
+                                                           brp_candidate* out, uint64_t out_cap, uint64_t* offsets,
+                                                           FilterArgs f, bool filtered) {
     extern __shared__ unsigned long long keys[];
     __shared__ uint64_t s_part[8];
+    __shared__ uint32_t s_fill;
     const uint32_t k = blockIdx.x, t = rank[k];
+    // the slot's written count: all its candidates, or those that pass the filter
+    auto written = [&](uint32_t u) { return filtered ? f.kept[u] : min(counts[u], capacity); };
     uint64_t acc = 0;
     for (uint32_t u = threadIdx.x; u < count; u += blockDim.x)
-        if (rank[u] < t) acc += min(counts[u], capacity);
+        if (rank[u] < t) acc += written(u);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+    if (threadIdx.x == 0) s_fill = 0u;
     __syncthreads();
     uint64_t off = 0;
 #pragma unroll
     for (int w = 0; w < 8; ++w) off += s_part[w];
-    const uint32_t c = min(counts[k], capacity);
+    const uint32_t all = min(counts[k], capacity), c = written(k);
+    const uint32_t s = filtered ? f.slot_series[k] : 0u;
     if (threadIdx.x == 0) {
         offsets[t] = off;
         if (t + 1 == count) offsets[count] = off + c;
     }
     const brp_candidate* src = cands + size_t(k) * capacity;
-    if (c > kCompactSortMax) {
-        const uint4* s4 = reinterpret_cast<const uint4*>(src);
-        uint4* d4 = reinterpret_cast<uint4*>(out);
-        for (uint32_t i = threadIdx.x; i < c; i += blockDim.x)
-            if (off + i < out_cap) d4[off + i] = s4[i];
+    if (c > kCompactSortMax) {  // unsorted (the host sorts); filtered lists in any order
+        for (uint32_t i = threadIdx.x; i < all; i += blockDim.x) {
+            const brp_candidate x = src[i];
+            if (filtered && !filter_keep(f, s, x)) continue;
+            const uint32_t at = filtered ? atomicAdd(&s_fill, 1u) : i;
+            if (off + at < out_cap) out[off + at] = x;
+        }
         return;
     }
     uint32_t P = 2;
     while (P < c) P <<= 1;
-    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
-        unsigned long long key = ~0ull;
-        if (i < c) {
+    if (filtered) {
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) keys[i] = ~0ull;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < all; i += blockDim.x) {
             const brp_candidate x = src[i];
-            key = (static_cast<unsigned long long>(x.level) << 55) | (static_cast<unsigned long long>(x.bin) << 32) |
-                  __float_as_uint(x.power);
+            if (filter_keep(f, s, x)) keys[atomicAdd(&s_fill, 1u)] = compact_key(x);
         }
-        keys[i] = key;
+    } else {
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) keys[i] = i < c ? compact_key(src[i]) : ~0ull;
     }
     __syncthreads();
     for (uint32_t w = 2; w <= P; w <<= 1) {
@@ -304,10 +319,11 @@ cudaError_t set_bank_compact_attributes(uint32_t capacity) {
 
 void launch_bank_compact(const uint32_t* counts, const brp_candidate* cands, uint32_t capacity, uint32_t count,
                          const uint32_t* rank, brp_candidate* out, uint64_t out_cap, uint64_t* offsets,
-                         cudaStream_t s) {
+                         const FilterArgs* filter, cudaStream_t s) {
     if (count)
         bank_compact_kernel<<<count, 256, compact_sort_size(capacity) * sizeof(unsigned long long), s>>>(
-            counts, cands, capacity, count, rank, out, out_cap, offsets);
+            counts, cands, capacity, count, rank, out, out_cap, offsets, filter ? *filter : FilterArgs{},
+            filter != nullptr);
 }
 
 }  // namespace brp

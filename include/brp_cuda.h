@@ -144,6 +144,15 @@ int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_
  * Used by the autotuner; the next run re-captures. */
 int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
                             uint32_t chains);
+/* Device pre-filter for the bank-wide toplist (src/workload.cpp:126-159, rows
+ * per harmonic level, one row per bin).  With rows > 0 brp_cuda_bank_run returns, per template, only
+ * the candidates whose power reaches the rows-th highest per-bin maximum power
+ * of their level among all candidates of the templates of the same series, and
+ * counts[t] is that kept count (overflow is still judged on the full count).
+ * Folding the kept candidates of a series into a toplist of `rows` rows per
+ * level in bank order gives the same final rows as folding all of them.
+ * rows = 0 (the default) returns every candidate.  The next run re-captures. */
+int brp_cuda_bank_set_toplist_filter(brp_bank* bank, uint32_t rows);
 /* Lists the compiled configurations: ids, sequence length L (pass 1: column
  * length L1, pass 2: row length L2) and kind (1 = pass 1, 2 = pass 2,
  * 3 = pass 1 whose first radix-16 stage runs on the tensor cores as split
