@@ -78,10 +78,13 @@ EXPORTS = (
     "brp_cuda_create", "brp_cuda_destroy", "brp_cuda_set_templates", "brp_cuda_run", "brp_cuda_snapshot",
     "brp_cuda_candidates", "brp_cuda_device_info", "brp_cuda_allocated_bytes", "brp_cuda_profile_counters",
     "brp_cuda_last_error", "brp_cuda_bank_create", "brp_cuda_bank_destroy", "brp_cuda_bank_set_series",
-    "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_configure", "brp_cuda_bank_set_toplist_filter", "brp_cuda_fast_configs", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
+    "brp_cuda_bank_run", "brp_cuda_bank_launch", "brp_cuda_bank_configure", "brp_cuda_bank_set_toplist_filter",
+    "brp_cuda_fast_configs", "brp_cuda_bank_profile", "brp_cuda_bank_stream", "brp_cuda_bank_kernels_per_run",
     "brp_cuda_bank_last_error", "brp_host_parameters", "brp_host_resampling_steps", "brp_host_search_parameters",
     "brp_toplist_create", "brp_toplist_destroy", "brp_toplist_thresholds", "brp_toplist_retain",
     "brp_toplist_final", "brp_toplist_fold", "brp_cuda_search_static", "brp_cuda_search_static_error",
+    "brp_cuda_preprocess", "brp_cuda_preprocess_dd", "brp_cuda_preprocess_error", "brp_host_read_zap",
+    "brp_host_zap_noise", "brp_host_error",
 )
 
 

@@ -140,6 +140,11 @@ struct PlainArgs {
 };
 // Records the plain pipeline on stream s; ev (optional, 5 events) brackets the 4 stages.
 void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev);
+// Its FFT stages: the forward complex FFT of the packed series (returns the
+// buffer holding Z, a or b) and the real post-process X_k, k = 0..M (power, if
+// given, |X_k|^2 / n for 0 < k < M and 0 at k = 0).
+float2* plain_complex_fft(float2* a, float2* b, const LengthPlan& lp, cudaStream_t s);
+void launch_plain_realpost(const float2* z, float2* fft, float* power, const LengthPlan& lp, cudaStream_t s);
 
 // Device toplist pre-filter of a bank run (toplist_filter.cu).  Per series s
 // the per-bin arrays of level h start at base[s] + h * half[s] (half = n/2).

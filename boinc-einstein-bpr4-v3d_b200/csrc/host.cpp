@@ -6,6 +6,7 @@
 // expressions round exactly where the reference's do.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -29,6 +30,7 @@ brp_resample_consts consts_of(const brp_params& p) {
 }  // namespace
 
 const char* brp_host_last_error() { return g_host_error.c_str(); }
+extern "C" const char* brp_host_error(void) { return g_host_error.c_str(); }
 
 extern "C" int brp_host_resampling_steps(brp_params* p) {
     // src/science.cpp:41-45: the largest steps with steps - offset(steps) < unpadded - 1.
@@ -248,5 +250,125 @@ extern "C" int brp_toplist_fold(brp_toplist* t, const brp_params* templates, con
         if (st) return st;
         off += counts[k];
     }
+    return BRP_OK;
+}
+
+// ---- RFI zap list and zap noise of the whitening step (src/workload.cpp:72-88) ----
+namespace {
+// The generator pair the reference takes from GSL (absent here): gsl_rng_taus2
+// and gsl_ran_gaussian_ziggurat.  Restated from the published algorithms:
+// L'Ecuyer's maximally equidistributed three-component Tausworthe generator
+// (Math. Comp. 65 (1996) 203-213) with the taus2 seeding (a 69069 LCG chain,
+// components raised to their minima 2, 8, 16, six warm-up draws), and Marsaglia
+// and Tsang's ziggurat (J. Stat. Softw. 5(8), 2000) for the normal with 128
+// layers, a 24-bit uniform and the sign and layer from the low byte.
+struct Taus2 {
+    uint32_t s1, s2, s3;
+    uint32_t next() {
+        s1 = ((s1 & 0xFFFFFFFEu) << 12) ^ (((s1 << 13) ^ s1) >> 19);
+        s2 = ((s2 & 0xFFFFFFF8u) << 4) ^ (((s2 << 2) ^ s2) >> 25);
+        s3 = ((s3 & 0xFFFFFFF0u) << 17) ^ (((s3 << 3) ^ s3) >> 11);
+        return s1 ^ s2 ^ s3;
+    }
+    double uniform() { return next() / 4294967296.0; }
+    explicit Taus2(uint32_t seed) {
+        if (!seed) seed = 1;
+        s1 = 69069u * seed;
+        if (s1 < 2) s1 += 2;
+        s2 = 69069u * s1;
+        if (s2 < 8) s2 += 8;
+        s3 = 69069u * s2;
+        if (s3 < 16) s3 += 16;
+        for (int i = 0; i < 6; ++i) next();
+    }
+};
+
+struct ZigguratTables {
+    static constexpr double R = 3.442619855899, V = 9.91256303526217e-3, M = 16777216.0;
+    double k[128], w[128], f[128];
+    ZigguratTables() {
+        double dn = R, tn = R;
+        const double q = V / std::exp(-0.5 * dn * dn);
+        k[0] = dn / q * M; k[1] = 0;
+        w[0] = q / M; w[127] = dn / M;
+        f[0] = 1.0; f[127] = std::exp(-0.5 * dn * dn);
+        for (int i = 126; i >= 1; --i) {
+            dn = std::sqrt(-2.0 * std::log(V / dn + std::exp(-0.5 * dn * dn)));
+            k[i + 1] = dn / tn * M;
+            tn = dn;
+            f[i] = std::exp(-0.5 * dn * dn);
+            w[i] = dn / M;
+        }
+    }
+};
+
+double gaussian(Taus2& r, double sigma) {
+    static const ZigguratTables z;
+    for (;;) {
+        const uint32_t bits = r.next();
+        const int i = int(bits & 0x7Fu);
+        const double sign = (bits & 0x80u) ? 1.0 : -1.0;
+        const uint32_t j = bits >> 8;
+        double x = j * z.w[i];
+        if (j < z.k[i]) return sign * sigma * x;
+        if (i == 0) {  // the tail beyond R
+            double y;
+            do {
+                x = -std::log(1.0 - r.uniform()) / ZigguratTables::R;
+                y = -std::log(1.0 - r.uniform());
+            } while (y + y < x * x);
+            return sign * sigma * (ZigguratTables::R + x);
+        }
+        if (z.f[i] + r.uniform() * (z.f[i - 1] - z.f[i]) < std::exp(-0.5 * x * x)) return sign * sigma * x;
+    }
+}
+}  // namespace
+
+extern "C" int brp_host_read_zap(const char* path, double* lower, double* upper, uint32_t cap, uint32_t* count) {
+    // src/workload.cpp:77-81, :88: whitespace-separated (lower, upper) pairs in Hz/seconds-normalised units.
+    if (!path || !count) return host_fail("null argument");
+    FILE* fp = std::fopen(path, "r");
+    if (!fp) return host_fail("cannot open zap list");
+    uint32_t k = 0;
+    double lo, hi;
+    int got;
+    while ((got = std::fscanf(fp, "%lf %lf", &lo, &hi)) == 2) {
+        if (!std::isfinite(lo + hi) || lo < 0 || hi < lo) { std::fclose(fp); return host_fail("invalid zap range"); }
+        if (k < cap) { if (lower) lower[k] = lo; if (upper) upper[k] = hi; }
+        ++k;
+    }
+    const bool clean = got == EOF && !std::ferror(fp);
+    std::fclose(fp);
+    if (!clean) return host_fail("malformed zap list");
+    *count = k;
+    return BRP_OK;
+}
+
+extern "C" int brp_host_zap_noise(uint32_t seed, uint32_t n, double sample_us, double padding, const double* lower,
+                                  const double* upper, uint32_t ranges, uint32_t* bins, float* values, uint32_t cap,
+                                  uint32_t* count) {
+    // src/workload.cpp:73-87: one taus2 stream seeded with the bits of the
+    // first decoded sample; per zapped bin a real then an imaginary Gaussian
+    // of sigma sqrt(2)/2 sqrt(padding), in the order of the ranges.
+    if (!count || (ranges && (!lower || !upper))) return host_fail("null argument");
+    Taus2 rng(seed);
+    const double seconds = double(n) * sample_us * 1e-6;
+    const uint64_t size = uint64_t(n) / 2 + 1;
+    const double sigma = std::sqrt(2.0) / 2 * std::sqrt(padding);
+    uint32_t k = 0;
+    for (uint32_t r = 0; r < ranges; ++r) {
+        if (!std::isfinite(lower[r] + upper[r]) || lower[r] < 0 || upper[r] < lower[r]) return host_fail("invalid zap range");
+        const double first = lower[r] * seconds + 0.5, last = upper[r] * seconds + 0.5;
+        if (last >= double(size)) return host_fail("zap exceeds Nyquist");
+        for (uint32_t i = uint32_t(first); i <= uint32_t(last); ++i) {
+            const float re = float(gaussian(rng, sigma)), im = float(gaussian(rng, sigma));
+            if (k < cap) {
+                if (bins) bins[k] = i;
+                if (values) { values[2 * k] = re; values[2 * k + 1] = im; }
+            }
+            ++k;
+        }
+    }
+    *count = k;
     return BRP_OK;
 }

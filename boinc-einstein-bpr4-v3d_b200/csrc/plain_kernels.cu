@@ -129,7 +129,7 @@ __global__ void plain_realpost(const float2* __restrict__ Z, float2* fft, float*
     float2 t = cmul(w, d);
     float2 X = make_float2(0.5f * (s.x + t.y), 0.5f * (s.y - t.x));
     fft[k] = X;
-    if (k < M) power[k] = k == 0 ? 0.f : (X.x * X.x + X.y * X.y) / float(n);
+    if (power && k < M) power[k] = k == 0 ? 0.f : (X.x * X.x + X.y * X.y) / float(n);
 }
 
 // harmonic.comp:14-35 (gather form).  grid.y = level.
@@ -178,17 +178,12 @@ inline uint32_t blocks_for(uint64_t n, uint32_t b) { return uint32_t((n + b - 1)
 
 }  // namespace
 
-void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
-    const LengthPlan& lp = *a.lp;
-    const brp_params& p = a.p;
-    if (ev) cudaEventRecord(ev[0], s);
-    const uint32_t rblocks = blocks_for(p.steps, kBlock);
-    plain_resample<<<rblocks, kBlock, 0, s>>>(a.input, p, a.raw, a.partial, a.status);
-    plain_mean<<<1, 1024, 0, s>>>(a.partial, rblocks, p.steps, a.mean);
-    plain_prepare<<<blocks_for(lp.M, kBlock), kBlock, 0, s>>>(a.raw, a.mean, a.a, p.steps, lp.M, lp.radix, lp.B);
-    if (ev) cudaEventRecord(ev[1], s);
-    // Radix-8 passes while at least three factors of two remain, then 4 or 2.
-    float2 *src = a.a, *dst = a.b;
+// Forward complex FFT of the M = radix * B packed points in `a` (in the
+// decimated order of plain_prepare), by global Stockham passes: radix 8 while at
+// least three factors of two remain, then 4 or 2, then the radix-3 combination.
+// `b` is scratch; returns the buffer that holds Z (a or b).
+float2* plain_complex_fft(float2* a, float2* b, const LengthPlan& lp, cudaStream_t s) {
+    float2 *src = a, *dst = b;
     const uint32_t seqs = lp.radix;
     uint32_t Ns = 1;
     while (Ns < lp.B) {
@@ -209,8 +204,25 @@ void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
         plain_radix3<<<blocks_for(lp.B, kBlock), kBlock, 0, s>>>(src, dst, lp.B, lp.fs_hi, lp.fs_lo);
         float2* t = src; src = dst; dst = t;
     }
-    plain_realpost<<<blocks_for(uint64_t(lp.M) + 1, kBlock), kBlock, 0, s>>>(src, a.fft, a.power, lp.M, lp.n, lp.rl_hi,
+    return src;
+}
+
+void launch_plain_realpost(const float2* z, float2* fft, float* power, const LengthPlan& lp, cudaStream_t s) {
+    plain_realpost<<<blocks_for(uint64_t(lp.M) + 1, kBlock), kBlock, 0, s>>>(z, fft, power, lp.M, lp.n, lp.rl_hi,
                                                                          lp.rl_lo);
+}
+
+void launch_plain(const PlainArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+    const LengthPlan& lp = *a.lp;
+    const brp_params& p = a.p;
+    if (ev) cudaEventRecord(ev[0], s);
+    const uint32_t rblocks = blocks_for(p.steps, kBlock);
+    plain_resample<<<rblocks, kBlock, 0, s>>>(a.input, p, a.raw, a.partial, a.status);
+    plain_mean<<<1, 1024, 0, s>>>(a.partial, rblocks, p.steps, a.mean);
+    plain_prepare<<<blocks_for(lp.M, kBlock), kBlock, 0, s>>>(a.raw, a.mean, a.a, p.steps, lp.M, lp.radix, lp.B);
+    if (ev) cudaEventRecord(ev[1], s);
+    float2* z = plain_complex_fft(a.a, a.b, lp, s);
+    launch_plain_realpost(z, a.fft, a.power, lp, s);
     if (ev) cudaEventRecord(ev[2], s);
     if (ev) cudaEventRecord(ev[3], s);
     plain_harmonic<<<dim3(blocks_for(p.fundamental, kBlock), 5), kBlock, 0, s>>>(a.power, p, a.summed, a.count,

@@ -85,16 +85,36 @@ __global__ void __launch_bounds__(1024) filter_select(FilterArgs f) {
             if ((key & mask) == prefix) atomicAdd(hist + ((key >> shift) & (nb - 1)), 1u);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t remaining = s_remaining, b = nb;
-            while (b > 0) {
-                --b;
-                if (hist[b] >= remaining) break;
-                remaining -= hist[b];
+        if (threadIdx.x < 32) {
+            // Walk the buckets from the highest down, 32 at a time: the bucket
+            // holding the remaining-th largest key is the first whose running
+            // count reaches `remaining`.
+            const uint32_t lane = threadIdx.x;
+            uint32_t remaining = s_remaining;
+            int found = 0;
+            for (int top = int(nb) - 1; top >= 0; top -= 32) {
+                const uint32_t h = hist[top - int(lane)];
+                uint32_t incl = h;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= uint32_t(o)) incl += v;
+                }
+                const uint32_t excl = incl - h;
+                const uint32_t hit = __ballot_sync(0xffffffffu, excl < remaining && incl >= remaining);
+                if (hit) {
+                    const int l = __ffs(hit) - 1;
+                    found = top - l;
+                    remaining -= __shfl_sync(0xffffffffu, excl, l);
+                    break;
+                }
+                remaining -= __shfl_sync(0xffffffffu, incl, 31);
             }
-            s_prefix = prefix | (b << shift);
-            s_mask = mask | ((nb - 1) << shift);
-            s_remaining = remaining;
+            if (lane == 0) {
+                s_prefix = prefix | (uint32_t(found) << shift);
+                s_mask = mask | ((nb - 1) << shift);
+                s_remaining = remaining;
+            }
         }
         __syncthreads();
     }

@@ -233,6 +233,44 @@ uint32_t brp_toplist_final(const brp_toplist* t, brp_bank_candidate* out);
 int brp_toplist_fold(brp_toplist* t, const brp_params* templates, const double* orbits,
                      const brp_candidate* candidates, const uint32_t* counts, uint32_t count);
 
+/* ---- Whitening and RFI zapping of an observation (brp::preprocess,
+ * src/workload.cpp:58-95) on the GPU ----
+ * decoded[samples] (host) is zero-padded to n (2^k or 3*2^k, 8192..3*2^22), real
+ * FFT, power, running median over `window` bins (even, <= n/2 and <= 4096 on
+ * the device), scaling of bin i + window/2 by sqrt(ln 2 / median_i), zapped
+ * bins (ranges zap_lower[z]..zap_upper[z] in the reference's units, x the
+ * observation length n * sample_us) replaced by Gaussian noise of sigma
+ * sqrt(padding / 2) drawn as the reference draws it (taus2 seeded with the bits
+ * of decoded[0], ziggurat), the first and last window/2 bins cleared, inverse
+ * real FFT and scaling by 1/sqrt(n); preprocessed[samples] (host) receives the
+ * result.  Errors follow the reference: BRP_E_ARGUMENT for an unsupported
+ * window, an invalid zap range or a zap beyond Nyquist, BRP_E_RESULT for an
+ * invalid median; brp_cuda_preprocess_error() gives the message. */
+int brp_cuda_preprocess(const float* decoded, uint32_t samples, uint32_t n, double sample_us, double padding,
+                        uint32_t window, const double* zap_lower, const double* zap_upper, uint32_t zap_count,
+                        float* preprocessed, int32_t device);
+/* As brp_cuda_preprocess from the DD sample bytes of brp::load_observation
+ * (src/workload.cpp:48-56): int8 samples, or (packed != 0) two 4-bit samples
+ * per byte, high nibble first, each float(double(b) / scale); decoded on the
+ * device (decoded[samples], host, optional, receives the decoded series). */
+int brp_cuda_preprocess_dd(const uint8_t* bytes, uint32_t samples, int32_t packed, double scale, uint32_t n,
+                           double sample_us, double padding, uint32_t window, const double* zap_lower,
+                           const double* zap_upper, uint32_t zap_count, float* decoded, float* preprocessed,
+                           int32_t device);
+const char* brp_cuda_preprocess_error(void);
+/* The zap list of src/workload.cpp:77-88: whitespace-separated (lower, upper)
+ * pairs; invalid ranges and trailing garbage are errors.  Writes at most cap
+ * pairs, *count = all pairs. */
+int brp_host_read_zap(const char* path, double* lower, double* upper, uint32_t cap, uint32_t* count);
+/* The zap noise of src/workload.cpp:73-87 for `ranges` zap ranges: per zapped
+ * bin (in the reference's order) bins[k] and values[2k], values[2k+1] (real,
+ * imaginary); at most cap written, *count = all. */
+int brp_host_zap_noise(uint32_t seed, uint32_t n, double sample_us, double padding, const double* lower,
+                       const double* upper, uint32_t ranges, uint32_t* bins, float* values, uint32_t cap,
+                       uint32_t* count);
+/* Message of the last failed brp_host_* call of this thread. */
+const char* brp_host_error(void);
+
 #ifdef __cplusplus
 }
 #endif

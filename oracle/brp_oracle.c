@@ -395,3 +395,204 @@ int oracle_rfft64(const float* x, uint32_t n, double* out_re, double* out_im) {
     free(re); free(im); free(cr); free(ci);
     return 0;
 }
+
+/* ---------------------------------------------------------------- whitening */
+/* In-place unnormalised complex DFT of length n = 2^k or 3*2^k in FP64:
+ * X_k = sum_j x_j exp(-+2 pi i jk / n) (minus for forward, plus for inverse). */
+int oracle_cfft64(double* re, double* im, uint32_t n, int inverse) {
+    uint32_t radix = single_bit(n) ? 1 : ((n % 3 == 0 && single_bit(n / 3)) ? 3 : 0);
+    if (!radix || n < 2) return fail("unsupported FFT length");
+    uint32_t m = n / radix;
+    double* cr = malloc(sizeof(double) * n);
+    double* ci = malloc(sizeof(double) * n);
+    double* tr = malloc(sizeof(double) * n);
+    double* ti = malloc(sizeof(double) * n);
+    if (!cr || !ci || !tr || !ti) { free(cr); free(ci); free(tr); free(ti); return fail("allocation failed"); }
+    for (uint32_t k = 0; k < n; ++k) {
+        double a = -2.0 * 3.14159265358979323846 * (double)k / (double)n;
+        cr[k] = cos(a); ci[k] = sin(a);
+    }
+    if (inverse) for (uint32_t j = 0; j < n; ++j) im[j] = -im[j];
+    for (uint32_t r = 0; r < radix; ++r)
+        for (uint32_t i = 0; i < m; ++i) { tr[r * m + i] = re[i * radix + r]; ti[r * m + i] = im[i * radix + r]; }
+    for (uint32_t r = 0; r < radix; ++r) fft2_inplace(tr + r * m, ti + r * m, m, cr, ci, radix);
+    for (uint32_t k = 0; k < n; ++k) {
+        double sr = 0, si = 0;
+        for (uint32_t r = 0; r < radix; ++r) {
+            uint32_t q = k % m;
+            uint64_t e = ((uint64_t)k * r) % n;
+            double ar = tr[r * m + q], ai = ti[r * m + q];
+            sr += ar * cr[e] - ai * ci[e]; si += ar * ci[e] + ai * cr[e];
+        }
+        re[k] = sr; im[k] = si;
+    }
+    if (inverse) for (uint32_t j = 0; j < n; ++j) im[j] = -im[j];
+    free(cr); free(ci); free(tr); free(ti);
+    return 0;
+}
+
+/* FFTW-style c2r: x_j = sum over all n bins of the Hermitian extension of
+ * X[0..n/2], imaginary parts of X_0 and X_{n/2} ignored; unnormalised. */
+int oracle_c2r64(const float* x_re, const float* x_im, uint32_t n, double* out) {
+    double* re = malloc(sizeof(double) * n);
+    double* im = malloc(sizeof(double) * n);
+    if (!re || !im) { free(re); free(im); return fail("allocation failed"); }
+    for (uint32_t k = 0; k <= n / 2; ++k) {
+        re[k] = x_re[k];
+        im[k] = (k == 0 || 2 * k == n) ? 0.0 : x_im[k];
+        if (k && k < n - k) { re[n - k] = x_re[k]; im[n - k] = -(double)x_im[k]; }
+    }
+    int st = oracle_cfft64(re, im, n, 1);
+    if (!st) for (uint32_t j = 0; j < n; ++j) out[j] = re[j];
+    free(re); free(im);
+    return st;
+}
+
+/* Running median: medians[i] = median of data[i .. i + window), i <= length -
+ * window; for an even window the mean of the two middle values, 0.5f * (a + b).
+ * The window's sorted copy is updated by one removal and one insertion per step. */
+int oracle_rngmed(const float* data, uint32_t length, uint32_t window, float* medians) {
+    if (!window || window > length) return fail("invalid running-median window");
+    float* w = malloc(sizeof(float) * window);
+    if (!w) return fail("allocation failed");
+    for (uint32_t i = 0; i < window; ++i) {  /* insertion sort of the first window */
+        uint32_t j = i;
+        while (j > 0 && w[j - 1] > data[i]) { w[j] = w[j - 1]; --j; }
+        w[j] = data[i];
+    }
+    for (uint32_t i = 0;; ++i) {
+        medians[i] = (window & 1) ? w[window / 2] : 0.5f * (w[window / 2 - 1] + w[window / 2]);
+        if (i + window >= length) break;
+        float out = data[i], in = data[i + window];
+        uint32_t j = 0;
+        while (j < window && !(w[j] == out || (w[j] != w[j] && out != out))) ++j; /* the leaving value */
+        if (j == window) { free(w); return fail("running median lost a value"); }
+        for (; j + 1 < window; ++j) w[j] = w[j + 1];
+        j = window - 1;
+        while (j > 0 && w[j - 1] > in) { w[j] = w[j - 1]; --j; }
+        w[j] = in;
+    }
+    free(w);
+    return 0;
+}
+
+void oracle_taus2_seed(oracle_taus2* r, uint32_t seed) {
+    if (!seed) seed = 1;
+    r->s1 = 69069u * seed; if (r->s1 < 2) r->s1 += 2;
+    r->s2 = 69069u * r->s1; if (r->s2 < 8) r->s2 += 8;
+    r->s3 = 69069u * r->s2; if (r->s3 < 16) r->s3 += 16;
+    for (int i = 0; i < 6; ++i) oracle_taus2_get(r);
+}
+
+uint32_t oracle_taus2_get(oracle_taus2* r) {
+    r->s1 = ((r->s1 & 4294967294u) << 12) ^ (((r->s1 << 13) ^ r->s1) >> 19);
+    r->s2 = ((r->s2 & 4294967288u) << 4) ^ (((r->s2 << 2) ^ r->s2) >> 25);
+    r->s3 = ((r->s3 & 4294967280u) << 17) ^ (((r->s3 << 3) ^ r->s3) >> 11);
+    return r->s1 ^ r->s2 ^ r->s3;
+}
+
+static double taus2_uniform(oracle_taus2* r) { return oracle_taus2_get(r) / 4294967296.0; }
+
+/* Marsaglia-Tsang ziggurat tables: 128 layers of area V, base layer plus tail
+ * beyond R, a 24-bit integer uniform. */
+static double zig_k[128], zig_w[128], zig_f[128];
+static int zig_ready = 0;
+static const double ZIG_R = 3.442619855899, ZIG_V = 9.91256303526217e-3, ZIG_M = 16777216.0;
+static void zig_init(void) {
+    double dn = ZIG_R, tn = ZIG_R, q = ZIG_V / exp(-0.5 * dn * dn);
+    zig_k[0] = dn / q * ZIG_M; zig_k[1] = 0;
+    zig_w[0] = q / ZIG_M; zig_w[127] = dn / ZIG_M;
+    zig_f[0] = 1.0; zig_f[127] = exp(-0.5 * dn * dn);
+    for (int i = 126; i >= 1; --i) {
+        dn = sqrt(-2.0 * log(ZIG_V / dn + exp(-0.5 * dn * dn)));
+        zig_k[i + 1] = dn / tn * ZIG_M;
+        tn = dn;
+        zig_f[i] = exp(-0.5 * dn * dn);
+        zig_w[i] = dn / ZIG_M;
+    }
+    zig_ready = 1;
+}
+
+double oracle_gaussian_ziggurat(oracle_taus2* r, double sigma) {
+    if (!zig_ready) zig_init();
+    for (;;) {
+        uint32_t bits = oracle_taus2_get(r);
+        int i = (int)(bits & 0x7Fu);
+        double sign = (bits & 0x80u) ? 1.0 : -1.0;
+        uint32_t j = bits >> 8;
+        double x = j * zig_w[i];
+        if (j < zig_k[i]) return sign * sigma * x;
+        if (i == 0) {
+            double y;
+            do {
+                x = -log(1.0 - taus2_uniform(r)) / ZIG_R;
+                y = -log(1.0 - taus2_uniform(r));
+            } while (y + y < x * x);
+            return sign * sigma * (ZIG_R + x);
+        }
+        if (zig_f[i] + taus2_uniform(r) * (zig_f[i - 1] - zig_f[i]) < exp(-0.5 * x * x)) return sign * sigma * x;
+    }
+}
+
+float oracle_dd_sample(const uint8_t* bytes, uint32_t i, int packed, double scale) {
+    /* src/workload.cpp:52-54 */
+    if (packed) return (float)((double)((i & 1) ? (bytes[i / 2] & 15) : (bytes[i / 2] >> 4)) / scale);
+    return (float)((double)(int8_t)bytes[i] / scale);
+}
+
+/* src/workload.cpp:58-95. */
+int oracle_preprocess(const float* decoded, uint32_t samples, uint32_t n, double sample_us, double padding,
+                      uint32_t window, const double* zap_lower, const double* zap_upper, uint32_t zap_count,
+                      float* preprocessed) {
+    if (!window || (window & 1) || window > n / 2) return fail("unsupported whitening window");
+    uint32_t size = n / 2 + 1;
+    float* time = calloc(n, sizeof(float));
+    double* xr = malloc(sizeof(double) * size);
+    double* xi = malloc(sizeof(double) * size);
+    float* fr = malloc(sizeof(float) * size);
+    float* fi = malloc(sizeof(float) * size);
+    float* power = malloc(sizeof(float) * size);
+    float* median = malloc(sizeof(float) * (size - window + 1));
+    double* back = malloc(sizeof(double) * n);
+    int st = 0;
+    if (!time || !xr || !xi || !fr || !fi || !power || !median || !back) { st = fail("allocation failed"); goto done; }
+    memcpy(time, decoded, sizeof(float) * samples);
+    if ((st = oracle_rfft64(time, n, xr, xi))) goto done;
+    for (uint32_t k = 0; k < size; ++k) { fr[k] = (float)xr[k]; fi[k] = (float)xi[k]; }
+    power[0] = 0;
+    for (uint32_t k = 1; k < size; ++k) { double re = fr[k], im = fi[k]; power[k] = (float)(re * re + im * im); }
+    if ((st = oracle_rngmed(power, size, window, median))) goto done;
+    for (uint32_t i = 0; i < size - window + 1; ++i) {
+        if (!(median[i] > 0) || !isfinite(median[i])) { st = fail("invalid whitening median"); goto done; }
+        float factor = (float)sqrt(0.693147180559945309417232121458 / median[i]);
+        fr[i + window / 2] *= factor;
+        fi[i + window / 2] *= factor;
+    }
+    {
+        uint32_t seed;
+        memcpy(&seed, &decoded[0], 4);
+        oracle_taus2 rng;
+        oracle_taus2_seed(&rng, seed);
+        double seconds = n * sample_us * 1e-6;
+        for (uint32_t z = 0; z < zap_count; ++z) {
+            double lower = zap_lower[z], upper = zap_upper[z];
+            if (!isfinite(lower + upper) || lower < 0 || upper < lower) { st = fail("invalid zap range"); goto done; }
+            double first = lower * seconds + 0.5, last = upper * seconds + 0.5;
+            if (last >= size) { st = fail("zap exceeds Nyquist"); goto done; }
+            for (uint32_t i = (uint32_t)first; i <= (uint32_t)last; ++i) {
+                double sigma = sqrt(2.0) / 2 * sqrt(padding);
+                float re = (float)oracle_gaussian_ziggurat(&rng, sigma), im = (float)oracle_gaussian_ziggurat(&rng, sigma);
+                fr[i] = re; fi[i] = im;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < window / 2; ++i) fr[i] = fi[i] = fr[size - i - 1] = fi[size - i - 1] = 0;
+    if ((st = oracle_c2r64(fr, fi, n, back))) goto done;
+    {
+        float factor = (float)(1.0 / sqrtf((float)n));
+        for (uint32_t i = 0; i < samples; ++i) preprocessed[i] = (float)back[i] * factor;
+    }
+done:
+    free(time); free(xr); free(xi); free(fr); free(fi); free(power); free(median); free(back);
+    return st;
+}

@@ -81,6 +81,28 @@ size_t oracle_toplist_final(const oracle_toplist* t, oracle_bank_candidate* out 
 /* FP64 reference DFT of a real float series of length n (2^k or 3*2^k); writes n/2+1 bins. */
 int oracle_rfft64(const float* x, uint32_t n, double* re, double* im);
 
+/* ---- whitening (src/workload.cpp:58-95) and DD decoding (:48-56) ----
+ * Parity notes: FFTW (FP32 r2c/c2r) is absent, the oracle transforms in FP64
+ * (the r2c output rounded to float, as the reference's std::complex<float>
+ * spectrum holds it); the historical rngmed.c is absent, oracle_rngmed defines
+ * the running median restated here (even window: 0.5f * (a + b) of the two
+ * middle values); GSL is absent, its taus2 generator and ziggurat Gaussian are
+ * restated from the published algorithms (L'Ecuyer 1996 with the taus2
+ * seeding; Marsaglia and Tsang 2000, 128 layers).  Those three are
+ * "parity unpinned"; the rest of the whitening is pinned against the
+ * reference's own preprocess compiled with these stand-ins (oracle/_ref). */
+int oracle_cfft64(double* re, double* im, uint32_t n, int inverse); /* in place, unnormalised */
+int oracle_c2r64(const float* x_re, const float* x_im, uint32_t n, double* out); /* sum over all n bins */
+int oracle_rngmed(const float* data, uint32_t length, uint32_t window, float* medians);
+typedef struct oracle_taus2 { uint32_t s1, s2, s3; } oracle_taus2;
+void oracle_taus2_seed(oracle_taus2* r, uint32_t seed);
+uint32_t oracle_taus2_get(oracle_taus2* r);
+double oracle_gaussian_ziggurat(oracle_taus2* r, double sigma);
+float oracle_dd_sample(const uint8_t* bytes, uint32_t i, int packed, double scale); /* workload.cpp:53-54 */
+int oracle_preprocess(const float* decoded, uint32_t samples, uint32_t n, double sample_us, double padding,
+                      uint32_t window, const double* zap_lower, const double* zap_upper, uint32_t zap_count,
+                      float* preprocessed);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus

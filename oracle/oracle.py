@@ -98,6 +98,17 @@ def lib():
         L.oracle_toplist_final.restype = ctypes.c_size_t
         L.oracle_toplist_final.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_rfft64.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_rngmed.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
+        L.oracle_taus2_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        L.oracle_taus2_get.restype = ctypes.c_uint32
+        L.oracle_taus2_get.argtypes = [ctypes.c_void_p]
+        L.oracle_gaussian_ziggurat.restype = ctypes.c_double
+        L.oracle_gaussian_ziggurat.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.oracle_dd_sample.restype = ctypes.c_float
+        L.oracle_dd_sample.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_double]
+        L.oracle_preprocess.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_uint32, ctypes.c_void_p]
         L.oracle_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
@@ -287,6 +298,10 @@ def ref():
                                          ctypes.c_double, ctypes.c_double, P]
         R.ref_toplist_final.restype = ctypes.c_uint32
         R.ref_toplist_final.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        R.ref_load_observation.argtypes = [ctypes.c_char_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_uint32]
+        R.ref_preprocess.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_void_p]
         _ref = R
     return _ref
 
@@ -367,3 +382,57 @@ class RefToplist:
         out = np.zeros(100, BANK_CANDIDATE)
         n = ref().ref_toplist_final(self._t, _fp(out))
         return out[:n].copy()
+
+
+# ---- whitening (src/workload.cpp:58-95) and DD decoding (:48-56) ----
+class Taus2(ctypes.Structure):
+    _fields_ = [("s1", ctypes.c_uint32), ("s2", ctypes.c_uint32), ("s3", ctypes.c_uint32)]
+
+
+def rngmed(data, window):
+    data = np.ascontiguousarray(data, np.float32)
+    out = np.empty(len(data) - window + 1, np.float32)
+    _check(lib().oracle_rngmed(_fp(data), len(data), window, _fp(out)))
+    return out
+
+
+def zap_noise(seed, count, sigma):
+    """`count` (real, imaginary) Gaussian pairs of the restated taus2/ziggurat stream."""
+    r = Taus2()
+    lib().oracle_taus2_seed(ctypes.byref(r), seed)
+    out = np.empty(2 * count, np.float32)
+    for k in range(2 * count):
+        out[k] = lib().oracle_gaussian_ziggurat(ctypes.byref(r), sigma)
+    return out
+
+
+def dd_decode(raw, samples, packed, scale):
+    raw = np.ascontiguousarray(raw, np.uint8)
+    return np.array([lib().oracle_dd_sample(_fp(raw), i, int(packed), scale) for i in range(samples)], np.float32)
+
+
+def preprocess(decoded, n, sample_us, padding, window, zap_lower=(), zap_upper=()):
+    decoded = np.ascontiguousarray(decoded, np.float32)
+    lo = np.ascontiguousarray(zap_lower, np.float64)
+    hi = np.ascontiguousarray(zap_upper, np.float64)
+    out = np.empty(len(decoded), np.float32)
+    _check(lib().oracle_preprocess(_fp(decoded), len(decoded), n, sample_us, padding, window, _fp(lo), _fp(hi),
+                                   len(lo), _fp(out)))
+    return out
+
+
+def ref_preprocess(decoded, n, sample_us, padding, zap_path, window):
+    decoded = np.ascontiguousarray(decoded, np.float32)
+    out = np.empty(len(decoded), np.float32)
+    _rcheck(ref().ref_preprocess(_fp(decoded), len(decoded), n, sample_us, padding, str(zap_path).encode(), window,
+                                 _fp(out)))
+    return out
+
+
+def ref_load_observation(path, padding):
+    """(sample_us, scale, samples, n), decoded samples, by the reference's loader."""
+    meta = np.zeros(4, np.float64)
+    _rcheck(ref().ref_load_observation(str(path).encode(), padding, _fp(meta), None, 0))
+    out = np.empty(int(meta[2]), np.float32)
+    _rcheck(ref().ref_load_observation(str(path).encode(), padding, _fp(meta), _fp(out), len(out)))
+    return (float(meta[0]), float(meta[1]), int(meta[2]), int(meta[3])), out

@@ -1,6 +1,6 @@
-/* Stand-in GSL declarations (GSL is not installed here).  Random numbers are
- * only used by whitening, outside the search path; gsl_rng_alloc returns NULL
- * so that path reports "GSL allocation failed".  TEST INFRASTRUCTURE ONLY. */
+/* Stand-in GSL declarations (GSL is not installed here).  The generator behind
+ * them is the oracle's restatement of taus2 (ref_shims.cpp).  TEST
+ * INFRASTRUCTURE ONLY. */
 #pragma once
 #ifdef __cplusplus
 extern "C" {

@@ -59,4 +59,24 @@ uint32_t ref_toplist_final(void* t, brp::BankCandidate* out) {
     std::memcpy(out, r.data(), r.size() * sizeof(brp::BankCandidate));
     return uint32_t(r.size());
 }
+// brp::load_observation (src/workload.cpp:29-57) of a gzip DD file: metadata
+// meta[4] = {sample_us, scale, samples, n}, decoded samples up to cap.
+int ref_load_observation(const char* path, double padding, double* meta, float* decoded, uint32_t cap) {
+    return guard([&] {
+        auto o = brp::load_observation(path, padding);
+        meta[0] = o.sample_us; meta[1] = o.scale; meta[2] = o.samples; meta[3] = o.n;
+        if (decoded) std::memcpy(decoded, o.decoded.data(), std::min<size_t>(cap, o.decoded.size()) * 4);
+    });
+}
+// brp::preprocess (src/workload.cpp:58-95) of a decoded series with a zap-list file.
+int ref_preprocess(const float* decoded, uint32_t samples, uint32_t n, double sample_us, double padding,
+                   const char* zap_path, uint32_t window, float* out) {
+    return guard([&] {
+        brp::Observation o;
+        o.sample_us = sample_us; o.padding = padding; o.samples = samples; o.n = n;
+        o.decoded.assign(decoded, decoded + samples);
+        brp::preprocess(o, zap_path, window);
+        std::memcpy(out, o.preprocessed.data(), size_t(samples) * 4);
+    });
+}
 }

@@ -31,3 +31,17 @@ def write_bank(path, orbits):
 
 def write_floats(path, x):
     np.ascontiguousarray(x, dtype=np.float32).tofile(path)
+
+
+def write_dd_bytes(path, raw, samples, sample_us, scale=1.0, dm=0.0):
+    """As write_dd with the sample bytes given: int8 samples (.binary) or two
+    4-bit samples per byte, high nibble first (.bin4)."""
+    header = bytearray(1168)
+    struct.pack_into("<d", header, 0, sample_us)
+    struct.pack_into("<d", header, 8, samples * sample_us * 1e-6)
+    struct.pack_into("<d", header, 13 * 8, dm)
+    struct.pack_into("<d", header, 14 * 8, scale)
+    struct.pack_into("<I", header, 128, samples)
+    with gzip.open(path, "wb") as f:
+        f.write(bytes(header))
+        f.write(np.asarray(raw, dtype=np.uint8).tobytes())
