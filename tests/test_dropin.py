@@ -7,6 +7,7 @@ dropin).  They apply the reference's own validation gates (src/main.cpp:55-94,
 src/workunit_main.cpp:103-122) and exit 0 only when every gate passes.  The
 binaries are built where the reference sources are present; elsewhere these
 tests are skipped."""
+import gzip
 import json
 import os
 import subprocess
@@ -94,3 +95,31 @@ def _rows(text):
         f = line.split()
         out.append((f[0], f[1], f[2], f[3], float(f[4]), float(f[5]), f[6]))
     return out
+
+
+def test_brp_workunit_accepts_gpu_whitening(tmp_path):
+    """The reference's own workunit driver whitens on the CPU (src/workunit_main.cpp:54,
+    brp::preprocess with the oracle's FFT/median/RNG stand-ins) and checks a
+    reference folder with its own gate (:57-62: decoded bit-exact, preprocessed
+    relative L2 < 1e-4); the folder holds the GPU's decoding and whitening."""
+    need(WORKUNIT)
+    from brp_b200 import whiten
+    dd, _, bank = _workunit_inputs(tmp_path)
+    zap = tmp_path / "zap.txt"
+    zap.write_text("223.0 223.05\n446.0 446.1\n1200 1200\n")
+    raw = np.frombuffer(gzip.open(dd).read()[1168:], np.uint8)
+    n = len(raw)
+    dec, pre = whiten.preprocess_dd(raw, n, False, 8.0, n, 128.0, 1.0, 1000, str(zap))
+    ref = tmp_path / "ref"
+    ref.mkdir()
+    dd_files.write_floats(ref / "decoded.f32", dec)
+    dd_files.write_floats(ref / "preprocessed.f32", pre)
+    out, met = tmp_path / "cand-white.txt", tmp_path / "met-white.jsonl"
+    cmd = [WORKUNIT, "--input", str(dd), "--bank", str(bank), "--zap", str(zap), "--padding", "1", "--f0", "400",
+           "--false-alarm", "0.08", "--window", "1000", "--output", str(out), "--metrics", str(met),
+           "--reference-dir", str(ref), "--cpu"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    m = json.loads(r.stdout.strip().splitlines()[-1])
+    print("workunit gate: decoded_l2 %g, preprocessed_l2 %g" % (m["decoded_l2"], m["preprocessed_l2"]))
+    assert m["decoded_l2"] == 0 and m["preprocessed_l2"] < 2e-6
