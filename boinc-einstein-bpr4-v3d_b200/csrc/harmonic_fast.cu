@@ -193,7 +193,8 @@ struct HCtx {
 };
 
 template <bool ALLV>
-__device__ __forceinline__ void sums_and_levels(const HCtx& c, LevelTail (&head)[4], LevelTail (&tail)[4]) {
+__device__ __forceinline__ void sums_and_levels(const HCtx& c, const float (&p16)[16], LevelTail (&head)[4],
+                                                LevelTail (&tail)[4]) {
     float s[16], t[16], v[16];
     auto mask = [&]() {
 #pragma unroll
@@ -209,8 +210,9 @@ __device__ __forceinline__ void sums_and_levels(const HCtx& c, LevelTail (&head)
     float* sm2 = c.summed ? c.summed + size_t(2) * c.fundamental : nullptr;
     float* sm3 = c.summed ? c.summed + size_t(3) * c.fundamental : nullptr;
     float* sm4 = c.summed ? c.summed + size_t(4) * c.fundamental : nullptr;
-    // stage A: s2 = P16 + P8
-    add_factor<16, true>(s, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
+    // stage A: s2 = P16 + P8 (P16 = the level-0 values)
+#pragma unroll
+    for (int r = 0; r < 16; ++r) s[r] = p16[r];
     add_factor<8, false>(s, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     mask();
     level_local<1, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[1], sm1, c.count, c.out, c.cap, c.status,
@@ -335,19 +337,22 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     // Bins outside [window, harmonic) (and the halo before bin 0) take the -1 sentinel.
     const bool all_valid = c.direct && c.i0 >= window && c.i0 + 16 <= harmonic;
 
-    // level 0: P[j], j = i0 + r
-    if (c.own) {
-        float p0[16];
-        if (c.direct) {
+    // P[16 m' + r]: level 0 (P[j], j = i0 + r) and factor 16 of the sums ((16 i + 8) >> 4 = i)
+    float p0[16];
+    if (c.direct) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 x = __ldg(reinterpret_cast<const float4*>(Pw + c.i0) + q);
-                p0[4 * q] = x.x; p0[4 * q + 1] = x.y; p0[4 * q + 2] = x.z; p0[4 * q + 3] = x.w;
-            }
-        } else {
-#pragma unroll
-            for (int r = 0; r < 16; ++r) p0[r] = c.i0 + r < M ? __ldg(Pw + c.i0 + r) : 0.f;
+        for (int q = 0; q < 4; ++q) {
+            const float4 x = __ldg(reinterpret_cast<const float4*>(Pw + c.i0) + q);
+            p0[4 * q] = x.x; p0[4 * q + 1] = x.y; p0[4 * q + 2] = x.z; p0[4 * q + 3] = x.w;
         }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int64_t gi = c.mp * 16 + r;
+            p0[r] = (gi >= 0 && gi < int64_t(M)) ? __ldg(Pw + gi) : 0.f;
+        }
+    }
+    if (c.own) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
             const uint32_t j = c.i0 + r;
@@ -359,8 +364,8 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     }
 
     LevelTail head[4], tail[4];
-    if (all_valid) sums_and_levels<true>(c, head, tail);
-    else sums_and_levels<false>(c, head, tail);
+    if (all_valid) sums_and_levels<true>(c, p0, head, tail);
+    else sums_and_levels<false>(c, p0, head, tail);
 
     // ---- u = 0 fundamental bins: previous thread's tail + own head
     const int lane = m & 31, warp = m >> 5;
