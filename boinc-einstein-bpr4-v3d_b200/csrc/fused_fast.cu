@@ -310,6 +310,13 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<512, 8, 256, 4, 8, 8, 8>::info(107),
         P1<512, 8, 256, 4, 16, 8, 4>::info(108),
         P1<1536, 4, 384, 2, 16, 8, 4, 3>::info(109),
+        P1<2048, 4, 512, 2, 16, 8, 16>::info(110),
+        P1<3072, 2, 384, 2, 16, 4, 3, 16>::info(115),
+        P1<3072, 2, 384, 2, 16, 3, 4, 16>::info(116),
+        P1<1024, 4, 256, 4, 16, 4, 16>::info(117),
+        P1<1024, 8, 512, 2, 16, 4, 16>::info(118),
+        P1<1536, 4, 384, 2, 16, 4, 3, 8>::info(119),
+        P1<512, 8, 256, 4, 16, 2, 16>::info(120),
     };
     append_pass1_tc_configs(v);
     return v;
