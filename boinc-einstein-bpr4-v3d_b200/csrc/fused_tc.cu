@@ -320,14 +320,16 @@ struct P1T {
 
 }  // namespace
 
-// Tensor-core pass-1 configurations: 111/112 transform columns of 2048 (M =
-// 2^21, n = 2^22) like 101, 113/114 columns of 3072 (n = 3 2^21) like 106;
-// the odd ids carry three BF16 parts per operand, the even ids two.
+// Tensor-core pass-1 configurations, each the tuned CUDA-core decomposition
+// with its first radix-16 stage on the tensor cores: 111/112 columns of 2048
+// (n = 2^22) as 16 x 8 x 16 like 110, 113/114 columns of 1536 (n = 3 2^21 with
+// rows of 2048) as 16 x 4 x 3 x 8 like 119; the odd ids carry three BF16 parts
+// per operand, the even ids two.
 void append_pass1_tc_configs(std::vector<FastPass>& v) {
-    v.push_back(P1T<2048, 4, 512, 2, 3, 16, 8>::info(111));
-    v.push_back(P1T<2048, 4, 512, 2, 2, 16, 8>::info(112));
-    v.push_back(P1T<3072, 2, 384, 2, 3, 16, 4, 3>::info(113));
-    v.push_back(P1T<3072, 2, 384, 2, 2, 16, 4, 3>::info(114));
+    v.push_back(P1T<2048, 4, 512, 2, 3, 8, 16>::info(111));
+    v.push_back(P1T<2048, 4, 512, 2, 2, 8, 16>::info(112));
+    v.push_back(P1T<1536, 4, 384, 2, 3, 4, 3, 8>::info(113));
+    v.push_back(P1T<1536, 4, 384, 2, 2, 4, 3, 8>::info(114));
 }
 
 }  // namespace brp

@@ -75,7 +75,7 @@ def test_tensor_core_pass1_configs_listed():
     from brp_b200 import tune
     from brp_b200._lib import fast_configs
     kinds = {i: (L, k) for i, L, k in fast_configs()}
-    for tc, base in ((111, 101), (112, 101), (113, 106), (114, 106)):
+    for tc, base in ((111, 110), (112, 110), (113, 119), (114, 119)):
         assert kinds[tc] == (kinds[base][0], 3)
     ids = {c[0] for c in tune.candidates(1 << 22) + tune.candidates(3 << 21)}
     assert ids and not ids & {111, 112, 113, 114}

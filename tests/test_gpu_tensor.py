@@ -1,7 +1,7 @@
 """Tensor-core form of pass 1 (compiled pass-1 configurations 111-114: the
 first radix-16 stage of the column FFTs as split-BF16 DFT products on the
 tensor cores, FP32 accumulation) against the FP64 FFT oracle and against the
-FP32 CUDA-core form of the same decomposition (101 for n = 2^22, 106 for
+FP32 CUDA-core form of the same decomposition (110 for n = 2^22, 119 for
 n = 3*2^21).
 
 Three BF16 parts per operand (111, 113) carry every bit of an FP32 operand and
@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 POWER_RTOL = {3: 2e-6, 2: 2e-5}
 THRESH_RTOL = {3: 1e-5, 2: 1e-4}
 # tensor-core id: (CUDA-core id of the same radix sequence, n, BF16 parts)
-TC = {111: (101, 1 << 22, 3), 112: (101, 1 << 22, 2), 113: (106, 3 << 21, 3), 114: (106, 3 << 21, 2)}
+TC = {111: (110, 1 << 22, 3), 112: (110, 1 << 22, 2), 113: (119, 3 << 21, 3), 114: (119, 3 << 21, 2)}
 
 
 def rel_rms(a, b):
@@ -78,7 +78,7 @@ def test_tensor_form_bank_mixed_radix():
     wl = synth.config4()
     n = wl.n[0]
     lists = {}
-    for p1 in (106, 113, 114):
+    for p1 in (119, 113, 114):
         bank = B.Bank(wl.n, [len(x) for x in wl.series], len(wl.templates), 8192)
         bank.set_series(0, wl.series[0])
         bank.configure(n, pass1=p1, pass2=0, group=16, chains=2)
@@ -86,11 +86,11 @@ def test_tensor_form_bank_mixed_radix():
         assert not status.any()
         lists[p1] = got
         bank.close()
-    total = sum(len(c) for c in lists[106])
+    total = sum(len(c) for c in lists[119])
     assert total > 0
     for p1, terms in ((113, 3), (114, 2)):
         ndiff = 0
-        for g, r, p in zip(lists[p1], lists[106], wl.templates):
+        for g, r, p in zip(lists[p1], lists[119], wl.templates):
             d, near = candidate_differences(g, r, p, THRESH_RTOL[terms])
             assert near
             ndiff += d
