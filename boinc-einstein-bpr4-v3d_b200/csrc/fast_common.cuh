@@ -218,9 +218,10 @@ __device__ __forceinline__ double gather(float2* sm, const float* __restrict__ i
 // Gather fused with the first Stockham pass (span 1, radix 16) when each
 // thread owns exactly one of its butterflies (L1 C = 16 THREADS): thread
 // t = j C + c gathers the 16 points n1 = j + r L1/16 of column c (the same
-// points, sums and snapshot writes as gather), transforms them in registers and
-// stores the 16 outputs at 16 j + m, so the samples never take a shared-memory
-// round trip before the first pass.
+// points, sums and snapshot writes as gather; indices of eight points, then
+// their 16 loads, twice), transforms them in registers and stores the 16
+// outputs at 16 j + m, so the samples never take a shared-memory round trip
+// before the first pass.
 template <int L1, int C, int THREADS, int STRIDE, int MODE>
 __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restrict__ in, const brp_params& P,
                                                uint32_t L2, uint32_t c0, float* raw, bool& oob) {
@@ -234,10 +235,10 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
     float2 x[16];
     float sum = 0.f;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        int jx[8];
+    for (int q = 0; q < 2; ++q) {
+        int jx[16];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
+        for (int b = 0; b < 16; ++b) {
             const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
             jx[b] = -1;
             if (ib < steps) {
@@ -248,11 +249,11 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
                 else oob = true;
             }
         }
-        float v[8];
+        float v[16];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) v[b] = jx[b] >= 0 ? __ldg(in + jx[b]) : 0.f;
+        for (int b = 0; b < 16; ++b) v[b] = jx[b] >= 0 ? __ldg(in + jx[b]) : 0.f;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < 8; ++b) {
             if (raw) {
                 const uint32_t ib = i + uint32_t(b) * istep;
                 if (ib < steps) raw[ib] = v[2 * b];
@@ -260,9 +261,9 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
             }
             sum += v[2 * b];
             sum += v[2 * b + 1];
-            x[4 * q + b] = make_float2(v[2 * b], v[2 * b + 1]);
+            x[8 * q + b] = make_float2(v[2 * b], v[2 * b + 1]);
         }
-        i += 4u * istep;
+        i += 8u * istep;
     }
     dft16(x);
     float2* dst = sm + c * STRIDE + ct_pos(16 * j);

@@ -22,6 +22,7 @@
 //      unnormalised inverse M-point DFT as conj(FFT(conj(2 Z))), even/odd
 //      samples from its real/imaginary parts, times float(1 / sqrtf(n)).
 // The window is limited to 4096 bins on the device (shared-memory sort).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -195,12 +196,20 @@ int preprocess_device(const float* d_decoded, float first_sample, uint32_t sampl
                                  reinterpret_cast<float*>(vals.data()), zc, &zc))
         return whiten_fail(BRP_E_ARGUMENT, brp_host_error());
     {
-        std::vector<uint32_t> last(size, UINT32_MAX);
-        for (uint32_t k = 0; k < zc; ++k) last[bins[k]] = k;
-        uint32_t w = 0;
+        // keep the last draw of each bin (overlapping ranges overwrite, as in the reference)
+        std::vector<std::pair<uint32_t, uint32_t>> order(zc);
+        for (uint32_t k = 0; k < zc; ++k) order[k] = {bins[k], k};
+        std::sort(order.begin(), order.end());
+        std::vector<uint32_t> keep_bins;
+        std::vector<float2> keep_vals;
         for (uint32_t k = 0; k < zc; ++k)
-            if (last[bins[k]] == k) { bins[w] = bins[k]; vals[w] = vals[k]; ++w; }
-        zc = w;
+            if (k + 1 == zc || order[k + 1].first != order[k].first) {
+                keep_bins.push_back(order[k].first);
+                keep_vals.push_back(vals[order[k].second]);
+            }
+        bins.swap(keep_bins);
+        vals.swap(keep_vals);
+        zc = uint32_t(bins.size());
     }
     LengthPlan lp;
     std::string e = make_length_plan(n, lp, s);

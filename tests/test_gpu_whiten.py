@@ -41,6 +41,15 @@ def test_preprocess_matches_oracle(oracle, n, samples, window):
     assert err <= REL_L2
 
 
+def test_overlapping_zap_ranges_take_the_last_draw(oracle):
+    n, samples = 1 << 18, 250000
+    x = series(samples, 6)
+    lo, hi = np.array([100.0, 100.2, 300.0]), np.array([100.4, 100.6, 300.1])  # the first two overlap
+    got = whiten.preprocess(x, n, SAMPLE_US, n / samples, 1000, (lo, hi))
+    want = oracle.preprocess(x, n, SAMPLE_US, n / samples, 1000, lo, hi)
+    assert rel_l2(got, want) <= REL_L2
+
+
 def test_dd_decoding_on_the_device(oracle):
     rng = np.random.default_rng(9)
     n, samples = 1 << 18, 240000
