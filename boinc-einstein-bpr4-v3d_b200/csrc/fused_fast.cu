@@ -317,6 +317,8 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<1024, 8, 512, 2, 16, 4, 16>::info(118),
         P1<1536, 4, 384, 2, 16, 4, 3, 8>::info(119),
         P1<512, 8, 256, 4, 16, 2, 16>::info(120),
+        P1<2048, 2, 256, 4, 16, 8, 16>::info(121),
+        P1<1536, 2, 192, 5, 16, 4, 3, 8>::info(122),
     };
     append_pass1_tc_configs(v);
     return v;
