@@ -150,3 +150,46 @@ def test_toplist_long_stream_with_and_without_ties(oracle, quantum):
     for f in finals[1:]:
         assert f.tobytes() == finals[0].tobytes()
     assert len(finals[0]) > 0
+
+
+def test_toplist_prefilter_rule_keeps_the_final_rows(oracle):
+    """The rule of the device toplist pre-filter (brp_cuda_bank_set_toplist_filter),
+    restated on the CPU: dropping every candidate below V, the 100th highest
+    per-bin maximum of its level over the whole stream, leaves the final toplist
+    unchanged -- for streams with repeated bins across templates, ties at V and
+    thresholds that vary per template."""
+    rng = np.random.default_rng(21)
+    p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
+    temps, orbs, cands = [], [], []
+    for t in range(120):
+        q = p.copy()
+        for h in range(5):
+            q.threshold[h] = p.threshold[h] * float(rng.uniform(0.9, 1.1))
+        c = _random_candidates(rng, q, 150)
+        c["bin"] = p.window + rng.integers(0, 400, len(c))  # few distinct bins: many repeats
+        c["power"] = np.round(c["power"] * 4) / 4            # ties, also at V
+        keep = c["power"] > np.asarray(list(q.threshold))[c["level"]]
+        c = c[keep]
+        _, first = np.unique(np.stack([c["level"], c["bin"]]), axis=1, return_index=True)
+        c = c[np.sort(first)]
+        c = c[np.lexsort((c["bin"], c["level"]))]
+        temps.append(q)
+        orbs.append((3600.0 + t, 0.01 * t, 0.1 * t))
+        cands.append(c)
+    allc = np.concatenate(cands)
+    V = np.zeros(5, np.float32)
+    for h in range(5):
+        lev = allc[allc["level"] == h]
+        best = {}
+        for b, pw in zip(lev["bin"].tolist(), lev["power"].tolist()):
+            best[b] = max(best.get(b, -1.0), pw)
+        maxima = sorted(best.values(), reverse=True)
+        V[h] = maxima[99] if len(maxima) >= 100 else 0.0
+    kept = [c[c["power"] >= V[c["level"]]] for c in cands]
+    assert sum(map(len, kept)) < sum(map(len, cands)) // 2
+    for make in (B.Toplist, oracle.Toplist):
+        full, pre = make(), make()
+        for q, o, c, k in zip(temps, orbs, cands, kept):
+            full.retain(c, *o, full.thresholds(q))
+            pre.retain(k, *o, pre.thresholds(q))
+        assert full.final().tobytes() == pre.final().tobytes()
