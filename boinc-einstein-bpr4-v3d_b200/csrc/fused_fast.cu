@@ -319,6 +319,7 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<512, 8, 256, 4, 16, 2, 16>::info(120),
         P1<2048, 2, 256, 4, 16, 8, 16>::info(121),
         P1<1536, 2, 192, 5, 16, 4, 3, 8>::info(122),
+        P1<2048, 8, 1024, 1, 16, 8, 16>::info(123),
     };
     append_pass1_tc_configs(v);
     return v;
