@@ -152,12 +152,16 @@ def test_toplist_long_stream_with_and_without_ties(oracle, quantum):
     assert len(finals[0]) > 0
 
 
-def test_toplist_prefilter_rule_keeps_the_final_rows(oracle):
+@pytest.mark.parametrize("shards", [1, 2, 3])
+def test_toplist_prefilter_rule_keeps_the_final_rows(oracle, shards):
     """The rule of the device toplist pre-filter (brp_cuda_bank_set_toplist_filter),
     restated on the CPU: dropping every candidate below V, the 100th highest
-    per-bin maximum of its level over the whole stream, leaves the final toplist
-    unchanged -- for streams with repeated bins across templates, ties at V and
-    thresholds that vary per template."""
+    per-bin maximum of its level over the candidates it sees, leaves the final
+    toplist unchanged -- for streams with repeated bins across templates, ties
+    at V and thresholds that vary per template.  With the bank split into
+    contiguous template shards (one per GPU) each shard takes its own V, which
+    is at most the whole bank's, and the ranks' kept lists folded in bank order
+    still give the same toplist."""
     rng = np.random.default_rng(21)
     p = B.search_parameters(1 << 20, 1 << 20, 128.0, 3600.0, 0.5, 0.1, 400.0, 0.08, 1000)
     temps, orbs, cands = [], [], []
@@ -176,16 +180,23 @@ def test_toplist_prefilter_rule_keeps_the_final_rows(oracle):
         temps.append(q)
         orbs.append((3600.0 + t, 0.01 * t, 0.1 * t))
         cands.append(c)
-    allc = np.concatenate(cands)
-    V = np.zeros(5, np.float32)
-    for h in range(5):
-        lev = allc[allc["level"] == h]
-        best = {}
-        for b, pw in zip(lev["bin"].tolist(), lev["power"].tolist()):
-            best[b] = max(best.get(b, -1.0), pw)
-        maxima = sorted(best.values(), reverse=True)
-        V[h] = maxima[99] if len(maxima) >= 100 else 0.0
-    kept = [c[c["power"] >= V[c["level"]]] for c in cands]
+    def threshold(lists):
+        allc = np.concatenate(lists)
+        V = np.zeros(5, np.float32)
+        for h in range(5):
+            lev = allc[allc["level"] == h]
+            best = {}
+            for b, pw in zip(lev["bin"].tolist(), lev["power"].tolist()):
+                best[b] = max(best.get(b, -1.0), pw)
+            maxima = sorted(best.values(), reverse=True)
+            V[h] = maxima[99] if len(maxima) >= 100 else 0.0
+        return V
+
+    kept = []
+    bounds = np.linspace(0, len(cands), shards + 1).astype(int)
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        V = threshold(cands[a:b])
+        kept += [c[c["power"] >= V[c["level"]]] for c in cands[a:b]]
     assert sum(map(len, kept)) < sum(map(len, cands)) // 2
     for make in (B.Toplist, oracle.Toplist):
         full, pre = make(), make()
