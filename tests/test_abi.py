@@ -79,3 +79,24 @@ def test_tensor_core_pass1_configs_listed():
         assert kinds[tc] == (kinds[base][0], 3)
     ids = {c[0] for c in tune.candidates(1 << 22) + tune.candidates(3 << 21)}
     assert ids and not ids & {111, 112, 113, 114}
+
+
+def test_argument_errors_of_the_whitening_and_filter_entry_points():
+    """Invalid arguments are rejected before any device work (no GPU needed):
+    a series longer than n, an unsupported length, a packed DD series of odd
+    length, a missing bank."""
+    import ctypes
+
+    import numpy as np
+    import pytest
+    from brp_b200 import whiten
+    from brp_b200._lib import lib
+    x = np.zeros(10000, np.float32)
+    with pytest.raises(B.BrpError, match="invalid observation"):
+        whiten.preprocess(x, 8192, 128.0, 1.0, 1000)
+    with pytest.raises(B.BrpError, match="2\\^k or 3\\*2\\^k"):
+        whiten.preprocess(x, 10000, 128.0, 1.0, 1000)
+    with pytest.raises(B.BrpError, match="invalid DD metadata"):
+        whiten.preprocess_dd(np.zeros(5000, np.uint8), 9999, True, 2.0, 16384, 128.0, 1.0, 1000)
+    L = lib()
+    assert L.brp_cuda_bank_set_toplist_filter(ctypes.c_void_p(0), 100) == 4
