@@ -79,7 +79,7 @@ def time_replays(bank, reps, flush):
     return total / reps
 
 
-def autotune(bank, templates, series_of=None, reps=3, groups=(8, 16), chains=(1, 2), cache_path=DEFAULT_CACHE,
+def autotune(bank, templates, series_of=None, reps=3, groups=(16, 32, 64, 128), chains=(1, 2), cache_path=DEFAULT_CACHE,
              use_cache=True):
     """Chooses the fastest configuration for every length class of `bank` on
     this workload; leaves the bank configured with it and returns
