@@ -22,6 +22,7 @@ select) with scipy's float32 real FFT standing in for FFTW, over all host cores.
 """
 import argparse
 import datetime
+import hashlib
 import json
 import os
 import statistics
@@ -112,8 +113,8 @@ def _cpu_init(series):
     O.ref() if O.ref_available() else O.lib()
 
 
-def _cpu_template(pbytes):
-    """One template through the reference CPU path; returns the candidate count."""
+def _cpu_search(pbytes):
+    """One template through the reference CPU path: (resampled series, candidates)."""
     import scipy.fft
     O = _W["O"]
     p = O.Params.from_buffer_copy(pbytes)
@@ -128,7 +129,20 @@ def _cpu_template(pbytes):
          * float(np.float32(1.0) / np.float32(n))).astype(np.float32)
     P[0] = 0
     S = O.ref_harmonic(P, p) if O.ref_available() else O.harmonic(P, p)
-    return len(O.select(S, p))
+    return r[: p.steps], O.select(S, p)
+
+
+def _cpu_template(pbytes):
+    """One template through the reference CPU path; returns the candidate count."""
+    return len(_cpu_search(pbytes)[1])
+
+
+def _cpu_check(pbytes):
+    """The reference CPU path's answer for one template, for the parity check:
+    (SHA-1 of the resampled samples below `steps`, candidate list)."""
+    import hashlib
+    r, c = _cpu_search(pbytes)
+    return hashlib.sha1(r.tobytes()).hexdigest(), c
 
 
 def cpu_pool(series, cores):
@@ -142,6 +156,55 @@ def time_cpu(pool, templates, sample):
     t0 = time.perf_counter()
     pool.map(_cpu_template, blobs, chunksize=1)
     return time.perf_counter() - t0
+
+
+def time_cpu_one_core(pool, templates, reps=3):
+    """Seconds per template on one host core (one worker process, scipy FFT
+    with one thread): the median of `reps` templates."""
+    times = []
+    for k in range(reps):
+        t0 = time.perf_counter()
+        pool.apply(_cpu_template, (bytes(templates[k % len(templates)]),))
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times)
+
+
+def reference_check(B, bank, pool, templates, orbits, sample, resampled_sha1):
+    """The reference's CPU path (its compiled resampling and harmonic sum, the
+    float32 FFT stand-in, select) on the first `sample` bank templates against
+    the bank's own full candidate lists for them (toplist pre-filter off):
+    template 0's resampled samples bit for bit (through brp::GPU's snapshot),
+    candidate (bin, level) keys equal except within 1e-5 relative of the
+    level's threshold (the FFTs differ by rounding), the largest relative power
+    difference of the shared keys, and the (bin, harmonics, template) order of
+    the final toplists folded from the two sets of lists."""
+    ref = pool.map(_cpu_check, [bytes(templates[k]) for k in range(sample)], chunksize=1)
+    bank.set_toplist_filter(0)
+    flat, offs, counts, status = bank.run_flat(B.Bank.params_array(templates[:sample]))
+    gpu = [flat[offs[t]:offs[t + 1]].copy() for t in range(sample)]
+    differ = near_threshold = 0
+    worst = 0.0
+    for t in range(sample):
+        thr = templates[t].threshold
+        kg = {(int(b), int(l)): float(v) for b, l, v in zip(gpu[t]["bin"], gpu[t]["level"], gpu[t]["power"])}
+        c = ref[t][1]
+        kr = {(int(b), int(l)): float(v) for b, l, v in zip(c["bin"], c["level"], c["power"])}
+        for k in set(kg) ^ set(kr):
+            differ += 1
+            v = kg.get(k, kr.get(k))
+            near_threshold += abs(v - thr[k[1]]) <= 1e-5 * thr[k[1]]
+        for k in set(kg) & set(kr):
+            worst = max(worst, abs(kg[k] - kr[k]) / max(abs(kr[k]), 1e-30))
+    tops = []
+    for lists in (gpu, [np.asarray(r[1]).view(B.CANDIDATE) for r in ref]):
+        top = B.Toplist().fold(templates[:sample], orbits[:sample], lists).final()
+        tops.append(list(zip(top["bin"].tolist(), top["harmonics"].tolist(), top["period"].tolist())))
+    return {"templates": sample, "status_words_clear": not bool(np.any(status)),
+            "resampled_template0_bit_exact": ref[0][0] == resampled_sha1,
+            "candidates_gpu": int(sum(len(c) for c in gpu)), "candidates_reference": int(sum(len(r[1]) for r in ref)),
+            "candidates_differ": differ, "candidates_differ_away_from_threshold": differ - int(near_threshold),
+            "max_power_rel_diff_shared": worst, "toplist_rows": len(tops[0]),
+            "toplist_row_order_equal": tops[0] == tops[1]}
 
 
 def host_cores():
@@ -331,6 +394,7 @@ def main():
     clocks.end()
     clock = clocks.stop()
     dev_ms = sum(step_ms)
+    launches_per_step = bank.kernels_per_run  # of the graph just timed
 
     # --- end to end through the public API (series H2D + candidates D2H + toplist)
     barrier()
@@ -354,9 +418,9 @@ def main():
 
     # the spectrum error of this build on the bench workload: one template's
     # power against an FP64 FFT of the same padded series
-    accuracy = None
+    accuracy = resampled_sha1 = None
     if rank == 0:
-        accuracy = spectrum_error(B, wl, my_templates[0])
+        accuracy, resampled_sha1 = spectrum_error(B, wl, my_templates[0])
 
     # plain per-template pipeline on the same GPU (comparator)
     plain = None
@@ -369,10 +433,15 @@ def main():
         sample = 64
         time_cpu(pool, wl.templates, min(cores, sample))
         secs = time_cpu(pool, wl.templates, sample)
-        pool.close()
+        one = time_cpu_one_core(pool, wl.templates)
         cpu = {"value": sample / secs, "unit": UNIT, "cores": cores, "kind": reference_kind(),
                "sample": "%d templates of the N=2^22 bank over %d processes (scipy float32 rfft for FFTW)" % (
-                   sample, cores)}
+                   sample, cores),
+               "one_core_value": 1.0 / one}
+        # parity of this run against the reference's CPU path (untimed)
+        accuracy["vs_reference_cpu"] = reference_check(B, bank, pool, my_templates, orbits, min(sample, count),
+                                                       resampled_sha1)
+        pool.close()
 
     if rank != 0:
         if dist:
@@ -398,7 +467,7 @@ def main():
                    "plan": plan},
         "e2e": {"value": total_templates * args.steps / (e2e_ms / 1000), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": bank.kernels_per_run * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": top_kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic * group if traffic else None,
@@ -482,6 +551,7 @@ def run_other_workload(args):
         step_ms.append(e0.elapsed_time(e1))
     clocks.end()
     clock = clocks.stop()
+    launches_per_step = bank.kernels_per_run  # of the graph just timed
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
@@ -500,6 +570,7 @@ def run_other_workload(args):
                    "l2": "flushed between steps (%d MiB write)" % (L2_FLUSH_BYTES >> 20),
                    "plan": plan},
         "e2e": {"value": count * args.steps / (e2e_ms / 1e3), "unit": UNIT},
+        "gpu_launches": launches_per_step * args.steps,
         "algorithmic_hbm_gbs": algo / (dev_ms / args.steps * 1e-3) / 1e9,
         "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": launches, "clocks": clock}), flush=True)
     bank.close()
@@ -517,7 +588,8 @@ def spectrum_error(B, wl, p):
     P = (X.real[: p.n // 2] ** 2 + X.imag[: p.n // 2] ** 2) / p.n
     P[0] = 0
     err = float(np.sqrt(np.sum((s.power - P) ** 2) / np.sum(P ** 2)))
-    return {"power_rel_rms_vs_fp64": err, "template": "bank template 0", "bar": 2e-6}
+    sha = hashlib.sha1(np.ascontiguousarray(s.resampled[: p.steps]).tobytes()).hexdigest()
+    return {"power_rel_rms_vs_fp64": err, "template": "bank template 0", "bar": 2e-6}, sha
 
 
 def time_plain(B, wl, templates):
