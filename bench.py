@@ -438,9 +438,13 @@ def main():
                "sample": "%d templates of the N=2^22 bank over %d processes (scipy float32 rfft for FFTW)" % (
                    sample, cores),
                "one_core_value": 1.0 / one}
-        # parity of this run against the reference's CPU path (untimed)
-        accuracy["vs_reference_cpu"] = reference_check(B, bank, pool, my_templates, orbits, min(sample, count),
-                                                       resampled_sha1)
+        # parity of this run against the reference's CPU path (untimed); a
+        # failure of the check is reported in the line, not swallowed
+        try:
+            accuracy["vs_reference_cpu"] = reference_check(B, bank, pool, my_templates, orbits,
+                                                           min(sample, count), resampled_sha1)
+        except Exception as e:
+            accuracy["vs_reference_cpu"] = {"error": "%s: %s" % (type(e).__name__, e)}
         pool.close()
 
     if rank != 0:
