@@ -484,11 +484,11 @@ extern "C" const char* brp_cuda_bank_last_error(const brp_bank* b) { return b ? 
 // Templates of one length class run in groups of `group` templates per launch;
 // the class's intermediate buffers hold one group.
 static uint32_t default_group(uint32_t n) {
-    // About 24 MiB of intermediates per template at n = 2^22; groups of 8
-    // keep a group's working set near the 126 MB L2.
-    if (n >= (1u << 22)) return 8;
-    if (n >= (1u << 20)) return 16;
-    return 32;
+    // Templates per launch when the caller does not configure the class: long
+    // launches amortise each kernel's partial last wave (the autotuner picks
+    // 64-128 on one B200).  Intermediates take 6n bytes per template: 3 GiB
+    // for 128 templates at n = 2^22.
+    return n >= (1u << 22) ? 128 : 64;
 }
 
 extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, const uint32_t* unpadded,

@@ -66,6 +66,17 @@ static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
     }
 }
 
+// The compiled pass pair a length takes when the caller names none: the pairs
+// the autotuner chose on one B200 for bank workloads of these lengths (n = 2^20,
+// 3*2^20, 2^22, 3*2^21).  Other lengths take the first compiled pair that fits.
+static void preferred_pair(uint32_t M, int& id1, int& id2) {
+    id1 = id2 = 0;
+    if (M == (1u << 19)) { id1 = 120; id2 = 202; }
+    if (M == (3u << 19)) { id1 = 119; id2 = 202; }
+    if (M == (1u << 21)) { id1 = 110; id2 = 202; }
+    if (M == (3u << 20)) { id1 = 119; id2 = 204; }
+}
+
 std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2) {
     const bool radix3 = !is_pow2(n);
     if (n < 64 || n > 3u * (1u << 22) || (radix3 && !(n % 3 == 0 && is_pow2(n / 3))))
@@ -80,19 +91,22 @@ std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2)
     // the power-of-two part of M), L1 = M / L2 <= 4096.
     // Compiled two-pass decomposition when one exists (rows of 1024 preferred).
     if (lp.M >= 4096 && fast1 >= 0 && fast2 >= 0) {
-        for (uint32_t l2 : {1024u, 512u, 2048u, 256u}) {
-            if (lp.M % l2 || lp.M / l2 > 4096) continue;
-            const FastPass* f1 = find_fast(fast_pass1_configs(), lp.M / l2, fast1);
-            const FastPass* f2 = find_fast(fast_pass2_configs(), l2, fast2);
-            if (!f1 || !f2 || l2 % f1->group || (lp.M / l2) % (2 * f2->group)) continue;
-            lp.fp1 = f1; lp.fp2 = f2;
-            lp.L1 = lp.M / l2; lp.L2 = l2; lp.C = f1->group; lp.R = f2->group;
-            lp.plan1 = f1->plan; lp.plan2 = f2->plan;
-            lp.fused = true;
-            if (f1->attr() != cudaSuccess || f2->attr() != cudaSuccess)
-                return "cannot enable the shared memory of the compiled fused kernels";
-            break;
-        }
+        int want1[2] = {fast1, fast1}, want2[2] = {fast2, fast2};
+        if (!fast1 && !fast2) preferred_pair(lp.M, want1[0], want2[0]);
+        for (int attempt = 0; attempt < 2 && !lp.fp1; ++attempt)
+            for (uint32_t l2 : {1024u, 512u, 2048u, 256u}) {
+                if (lp.M % l2 || lp.M / l2 > 4096) continue;
+                const FastPass* f1 = find_fast(fast_pass1_configs(), lp.M / l2, want1[attempt]);
+                const FastPass* f2 = find_fast(fast_pass2_configs(), l2, want2[attempt]);
+                if (!f1 || !f2 || l2 % f1->group || (lp.M / l2) % (2 * f2->group)) continue;
+                lp.fp1 = f1; lp.fp2 = f2;
+                lp.L1 = lp.M / l2; lp.L2 = l2; lp.C = f1->group; lp.R = f2->group;
+                lp.plan1 = f1->plan; lp.plan2 = f2->plan;
+                lp.fused = true;
+                if (f1->attr() != cudaSuccess || f2->attr() != cudaSuccess)
+                    return "cannot enable the shared memory of the compiled fused kernels";
+                break;
+            }
     }
     if (lp.M >= 4096 && !lp.fp1) {
         uint32_t a = ilog2(lp.B);
