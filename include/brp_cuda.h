@@ -148,7 +148,7 @@ int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t p
  * per harmonic level, one row per bin).  With rows > 0 brp_cuda_bank_run returns, per template, only
  * the candidates whose power reaches the rows-th highest per-bin maximum power
  * of their level among all candidates of the templates of the same series, and
- * counts[t] is that kept count (overflow is still judged on the full count).
+ * counts[t] is that kept count (overflow is still decided on the full count).
  * Folding the kept candidates of a series into a toplist of `rows` rows per
  * level in bank order gives the same final rows as folding all of them.
  * rows = 0 (the default) returns every candidate.  The next run re-captures. */
