@@ -400,10 +400,17 @@ def main():
     barrier()
     t0 = time.perf_counter()
     top = B.Toplist()
+    all_tarr = B.Bank.params_array(wl.templates) if rank == 0 and world > 1 else None
+    all_orbits = np.asarray(wl.orbits, np.float64)
     for _ in range(args.steps):
         flat, offs, counts, status = e2e_step()
         if world == 1:
             top.fold(tarr, orbits, flat, counts)
+        else:
+            # every rank's kept lists to rank 0, folded there in bank order
+            merged = shard.gather_candidates([flat[offs[t]:offs[t + 1]] for t in range(count)], begin)
+            if rank == 0:
+                top.fold(all_tarr, all_orbits, merged)
     torch.cuda.synchronize()
     e2e_ms = 1000 * (time.perf_counter() - t0)
     barrier()
