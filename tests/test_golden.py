@@ -99,3 +99,41 @@ def test_chisq_inverse_roundtrip(oracle):
             assert abs(oracle.chisq_Q(x, nu) / q - 1) < 1e-12
     # closed form at nu = 2: Q = exp(-x/2)
     assert abs(oracle.chisq_Q(10.0, 2) - np.exp(-5.0)) < 1e-15
+
+
+WHITENING = os.path.join(os.path.dirname(GOLDEN), "whitening_vectors.npz")
+
+
+@pytest.fixture(scope="module")
+def W():
+    return np.load(WHITENING)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_whitening_golden(oracle, W, k):
+    """brp::preprocess (src/workload.cpp:58-95) by the oracle against the
+    reference's own output (tests/golden/make_whitening_golden.py); the zap
+    rows go through the product's zap-list reader first."""
+    import tempfile
+
+    from brp_b200 import whiten
+    n, samples, window, padding = W["pre_case_%d" % k]
+    rows = W["pre_zap_%d" % k]
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "zap.txt")
+        with open(path, "w") as f:
+            f.write("".join("%r %r\n" % (float(a), float(b)) for a, b in rows))
+        lo, hi = whiten.read_zap(path)
+    assert np.array_equal(lo, rows[:, 0]) and np.array_equal(hi, rows[:, 1])
+    got = oracle.preprocess(W["pre_input_%d" % k], int(n), 128.0, float(padding), int(window), lo, hi)
+    assert np.array_equal(got.view(np.uint32), W["pre_output_%d" % k].view(np.uint32))
+
+
+@pytest.mark.parametrize("name,packed", [("int8", False), ("packed", True)])
+def test_dd_decoding_golden(oracle, W, name, packed):
+    """DD sample decoding of brp::load_observation (src/workload.cpp:48-56):
+    bit-exact, with the reference loader's sample count and scale."""
+    sample_us, scale, samples, n = W["dd_meta_" + name]
+    assert sample_us == 128.0 and scale == 3.5
+    got = oracle.dd_decode(W["dd_raw_" + name], int(samples), packed, scale)
+    assert np.array_equal(got.view(np.uint32), W["dd_decoded_" + name].view(np.uint32))

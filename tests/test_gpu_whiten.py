@@ -4,6 +4,8 @@ preprocess with the same FFT/median/RNG stand-ins): relative L2 of the
 preprocessed series within 2e-6 (the reference's own gate against the authentic
 application is 1e-4, src/workunit_main.cpp:62); zapped bins carry the same
 noise; DD samples decoded on the device bit-exactly; the reference's errors."""
+import os
+
 import numpy as np
 import pytest
 
@@ -72,3 +74,25 @@ def test_preprocess_errors():
         whiten.preprocess(x, n, SAMPLE_US, n / 60000, 1000, ([0.0], [1e9]))
     with pytest.raises(B.BrpError, match="invalid whitening median"):
         whiten.preprocess(np.zeros(60000, np.float32), n, SAMPLE_US, n / 60000, 1000)
+
+
+def test_against_reference_golden():
+    """The device whitening against the reference's own preprocess output
+    (tests/golden/whitening_vectors.npz, made by src/workload.cpp compiled with
+    the oracle's stand-ins) within the same relative L2 bar, and the device DD
+    decoding bit-exact against the reference loader's samples."""
+    W = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "whitening_vectors.npz"))
+    for k in (0, 1):
+        n, samples, window, padding = W["pre_case_%d" % k]
+        rows = W["pre_zap_%d" % k]
+        got = whiten.preprocess(W["pre_input_%d" % k], int(n), SAMPLE_US, float(padding), int(window),
+                                (rows[:, 0], rows[:, 1]))
+        err = rel_l2(got, W["pre_output_%d" % k])
+        print("golden case %d (n=%d): preprocessed relative L2 vs the reference %.3g" % (k, int(n), err))
+        assert err <= REL_L2
+    for name, packed in (("int8", False), ("packed", True)):
+        sample_us, scale, samples, _ = W["dd_meta_" + name]
+        n = 8192  # the device whitening's shortest length
+        dec, _ = whiten.preprocess_dd(W["dd_raw_" + name], int(samples), packed, float(scale), n, float(sample_us),
+                                      n / samples, 1000)
+        assert np.array_equal(dec.view(np.uint32), W["dd_decoded_" + name].view(np.uint32))
