@@ -457,6 +457,22 @@ struct brp_bank {
         allocations.push_back(*p);
         return BRP_OK;
     }
+    // Frees one buffer of alloc() (the caller has synchronised the stream and
+    // dropped every graph that references it).
+    void release(void* p) {
+        auto it = std::find(allocations.begin(), allocations.end(), p);
+        if (it == allocations.end()) return;
+        cudaFree(p);
+        allocations.erase(it);
+    }
+    // The captured graph references the class buffers, plan tables and filter
+    // state of the last run; a change to any of them drops it, so that
+    // brp_cuda_bank_launch cannot replay a stale graph and the next run captures.
+    void drop_graph() {
+        if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+        if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+        graph_key.clear();
+    }
     ~brp_bank() {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
@@ -760,17 +776,20 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
     brp_bank::ClassBuffers& cb = b->classes.at(n);
     const uint32_t g = group ? std::min(group, b->max_templates) : cb.group;
     const uint32_t ch = chains ? std::min(chains, 2u) : cb.chains;
+    b->drop_graph();  // it references the plan tables freed below
     if (g * ch > cb.capacity || lp.blocks1() > cb.partial_per_template) {
-        // grow the class buffers
+        // grow the class buffers; the old ones are freed once the new ones exist
         brp_bank::ClassBuffers nb;
         nb.capacity = std::max(g * ch, cb.capacity);
         nb.partial_per_template = std::max(lp.blocks1(), cb.partial_per_template);
         if ((st = b->alloc(&nb.work, size_t(nb.capacity) * lp.M, "work")) ||
             (st = b->alloc(&nb.power, size_t(nb.capacity) * lp.M, "power")) ||
             (st = b->alloc(&nb.partial, size_t(nb.capacity) * nb.partial_per_template, "partial"))) {
+            b->release(nb.work); b->release(nb.power); b->release(nb.partial);
             free_length_plan(lp);
             return st;
         }
+        b->release(cb.work); b->release(cb.power); b->release(cb.partial);
         cb.work = nb.work; cb.power = nb.power; cb.partial = nb.partial;
         cb.capacity = nb.capacity; cb.partial_per_template = nb.partial_per_template;
     }
@@ -778,7 +797,6 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
     cb.chains = ch;
     free_length_plan(it->second);
     it->second = lp;
-    b->graph_key.clear();
     return BRP_OK;
 }
 
@@ -818,7 +836,7 @@ extern "C" int brp_cuda_bank_set_toplist_filter(brp_bank* b, uint32_t rows) {
     }
     b->filter_rows = rows;
     b->filter.rows = rows;
-    b->graph_key.clear();
+    b->drop_graph();
     return BRP_OK;
 }
 
@@ -837,12 +855,14 @@ extern "C" int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* 
 }
 
 extern "C" int brp_cuda_bank_launch(brp_bank* b) {
-    if (!b || !b->exec) return set_thread_error(BRP_E_ARGUMENT, "no captured bank graph");
+    if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    if (!b->exec) return b->fail(BRP_E_ARGUMENT, "no captured bank graph (run the bank after configuring it)");
     return b->cuda(cudaGraphLaunch(b->exec, b->stream), "graph launch");
 }
 
 extern "C" int brp_cuda_bank_profile(brp_bank* b, double* kernel_ms, uint32_t* launches) {
-    if (!b || !kernel_ms || !b->last_count) return set_thread_error(BRP_E_ARGUMENT, "no bank run to profile");
+    if (!b || !kernel_ms) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (!b->last_count) return b->fail(BRP_E_ARGUMENT, "no bank run to profile");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
     KernelEvents prof;

@@ -141,7 +141,8 @@ int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_
 /* Selects the kernels of one length class: compiled pass-1 / pass-2
  * configuration ids (0 = default, -1 = generic kernels), templates per
  * launch and independent launch chains in the graph (1 or 2; 0 = keep).
- * Used by the autotuner; the next run re-captures. */
+ * Used by the autotuner; the next run re-captures.  Buffers that a larger
+ * group replaces are freed. */
 int brp_cuda_bank_configure(brp_bank* bank, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
                             uint32_t chains);
 /* Device pre-filter for the bank-wide toplist (src/workload.cpp:126-159, rows
@@ -161,7 +162,9 @@ int brp_cuda_bank_set_toplist_filter(brp_bank* bank, uint32_t rows);
 int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* kinds, uint32_t cap);
 /* Device-only replay of the last brp_cuda_bank_run's graph (no host copies,
  * no wait): the throughput kernel time is measured around this by the caller
- * with events on brp_cuda_bank_stream(). */
+ * with events on brp_cuda_bank_stream().  brp_cuda_bank_configure and
+ * brp_cuda_bank_set_toplist_filter drop the graph: until the next run this
+ * returns BRP_E_ARGUMENT. */
 int brp_cuda_bank_launch(brp_bank* bank);
 void* brp_cuda_bank_stream(brp_bank* bank);
 /* Replays the last run's kernels eagerly with an event pair around each launch

@@ -119,3 +119,32 @@ def test_resample_out_of_range_reported():
         bank.run([bad])
     assert e.value.status[0] & B.STATUS_RESAMPLE_OOB
     bank.close()
+
+
+def test_configure_drops_the_graph_and_frees_replaced_buffers():
+    """brp_cuda_bank_configure drops the captured graph (a replay before the
+    next run is refused instead of reading replaced plan tables) and frees the
+    class buffers it replaces when a larger group needs more: growing a 2^20
+    class (6 MiB of intermediates per template) from 64 to 128 templates costs
+    the difference, not a second full set."""
+    import torch
+    wl = synth.bank_workload("configure", [1 << 20], [64], [1], seed=8)
+    bank = B.Bank(wl.n, [len(x) for x in wl.series], 64, 8192)
+    bank.set_series(0, wl.series[0])
+    first, _, _ = bank.run(wl.templates)
+    bank.launch()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    bank.configure(1 << 20, pass1=0, pass2=0, group=64, chains=2)  # 128 templates' buffers
+    free1 = torch.cuda.mem_get_info()[0]
+    with pytest.raises(B.BrpError, match="no captured bank graph"):
+        bank.launch()
+    again, _, _ = bank.run(wl.templates)
+    bank.launch()
+    torch.cuda.synchronize()
+    bank.close()
+    grown = (free0 - free1) / (1 << 20)
+    print("configure 64 -> 2 x 64 templates: %.0f MiB more device memory" % grown)
+    assert 300 <= grown <= 500  # 64 x 6 MiB = 384 MiB (not 768)
+    for a, b in zip(first, again):
+        assert np.array_equal(a, b)
