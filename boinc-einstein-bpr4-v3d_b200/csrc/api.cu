@@ -751,7 +751,7 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
         const uint32_t t = order[k];
         const uint32_t kept = b->filter_rows ? b->h_kept[k] : std::min(b->h_counts[k], b->capacity);
         counts[t] = b->filter_rows ? kept : b->h_counts[k];
-        status[t] = h_status[k] | (b->h_counts[k] > b->capacity ? BRP_STATUS_OVERFLOW : 0u);
+        status[t] = h_status[k] | (b->h_counts[k] > b->capacity ? uint32_t(BRP_STATUS_OVERFLOW) : 0u);
         if (status[t]) bad = true;
         const uint64_t first = b->h_offsets[t];
         if (out && kept > kCompactSortMax && first + kept <= out_cap) sort_candidates(out + first, kept);
