@@ -12,13 +12,19 @@ Reported (one JSON line, rank 0):
   e2e        the same metric through the public API (Bank.run) with the
              series copied from pinned host memory every step, candidates copied
              back and folded into the bank-wide toplist on the host
-  roofline   the dominant kernel's algorithmic bytes / its device time
+  roofline   the dominant kernel's algorithmic bytes / its device time, and
+             its ncu DRAM bytes / its device time
   plain      templates/s of the step-by-step per-template pipeline, same GPU
-  cpu_baseline  the reference CPU path on a bounded sample (rank 0, N = 1)
+  cpu_baseline  the reference CPU path over the whole bank once (rank 0, N = 1)
 
 `--impl reference` times the reference's own CPU implementation of the path
 (oracle/_ref: src/science.cpp resampling, the harmonic summing restatement,
-select) with scipy's float32 real FFT standing in for FFTW, over all host cores.
+select) with scipy's float32 real FFT standing in for FFTW, over all host
+cores, on the same bank: its templates come from the reference's own compiled
+search_parameters (src/workload.cpp:108-125), and each timed step searches the
+whole 512-template bank (a rotating sample of it only when the steps would not
+fit REF_TIMED_BUDGET_S).  The reference process loads none of this
+repository's CUDA library.
 """
 import argparse
 import datetime
@@ -44,6 +50,7 @@ CAPACITY = 8192
 METRIC = "orbital templates/s at N=2^22 on 1 B200 (batched bank search)"
 UNIT = "templates/s"
 L2_FLUSH_BYTES = 512 << 20
+REF_TIMED_BUDGET_S = 240.0  # bound of the reference arm's timed region (all steps)
 # Algorithmic HBM bytes per template (per kernel) at length n: pass 1 gathers the
 # series (4n) and writes the four-step intermediate (4n); pass 2 reads it (4n) and
 # writes the power spectrum (2n); harmonic summing reads the power spectrum (2n).
@@ -64,6 +71,8 @@ def parse():
                    help="pass1,pass2,group,chains: use this configuration instead of the autotuner")
     a.add_argument("--toplist-rows", type=int, default=100,
                    help="device toplist pre-filter rows per level (0: return every candidate)")
+    a.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                   help="process-group backend of the multi-rank run (the search has no data-path collective)")
     a.add_argument("--workload", default="bank", choices=["bank", "mixed-radix", "uneven"],
                    help="bank: N=2^22, 512 templates (the headline); mixed-radix: N=3*2^21, 128 templates; "
                         "uneven: 1024 templates over N in {2^20, 3*2^20, 2^22} (1 GPU, documentation runs)")
@@ -96,9 +105,20 @@ def measured_traffic():
 
 
 # ------------------------------------------------------------------ workload
-def workload(total_templates):
+def workload(total_templates, search=None):
     from brp_b200 import synth
-    return synth.bank_workload("bank-2^22", [N], [total_templates], [3], seed=3)
+    return synth.bank_workload("bank-2^22", [N], [total_templates], [3], seed=3, search=search)
+
+
+def workload_name(templates):
+    return "bank search, N=2^22, %d templates per GPU, 3 injected pulsars" % templates
+
+
+def reference_search():
+    """The reference's own search_parameters (oracle/_ref, compiled from
+    src/workload.cpp), else the oracle's restatement of it."""
+    from oracle import oracle as O
+    return O.ref_search_parameters if O.ref_available() else O.search_parameters
 
 
 # --------------------------------------------------------------- CPU baseline
@@ -151,8 +171,9 @@ def cpu_pool(series, cores):
     return ctx.Pool(cores, initializer=_cpu_init, initargs=(series,))
 
 
-def time_cpu(pool, templates, sample):
-    blobs = [bytes(templates[k % len(templates)]) for k in range(sample)]
+def time_cpu(pool, templates, sample, start=0):
+    """Seconds for `sample` templates (from `start`, wrapping) over the pool."""
+    blobs = [bytes(templates[(start + k) % len(templates)]) for k in range(sample)]
     t0 = time.perf_counter()
     pool.map(_cpu_template, blobs, chunksize=1)
     return time.perf_counter() - t0
@@ -279,26 +300,42 @@ class Clocks:
 
 # --------------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
+    """The reference's CPU path on the bench bank, all host cores, rank 0 only.
+    Each timed step searches the per-GPU bank (all args.templates templates;
+    at N > 1 the first args.templates of the N-GPU bank), unless K such steps
+    would exceed REF_TIMED_BUDGET_S, in which case each step searches a
+    rotating sample of it (stated in config.workload).  Warm-up steps search
+    one template per worker."""
     if rank != 0:
         return
-    wl = workload(args.templates)
+    wl = workload(args.templates * world, search=reference_search())
+    bank = wl.templates[:args.templates]
     cores = host_cores()
     pool = cpu_pool(wl.series[0], cores)
-    sample = max(cores, 16)
-    for _ in range(max(args.warmup, 1)):
-        time_cpu(pool, wl.templates, min(sample, cores))
-    times = [time_cpu(pool, wl.templates, sample) for _ in range(args.steps)]
+    warm = [time_cpu(pool, bank, cores, k * cores) for k in range(max(args.warmup, 1))]
+    rate = cores / min(warm)  # templates/s, from the fastest warm-up step
+    per_step = len(bank)
+    if args.steps * per_step / rate > REF_TIMED_BUDGET_S:
+        per_step = max(cores, int(REF_TIMED_BUDGET_S * rate / args.steps) // cores * cores)
+    times = [time_cpu(pool, bank, per_step, k * per_step) for k in range(args.steps)]
     pool.close()
     total = sum(times)
-    value = sample * args.steps / total
+    value = per_step * args.steps / total
     kind = reference_kind()
+    name = workload_name(args.templates)
+    if per_step < len(bank):
+        name += " (reference: a rotating sample of %d of the %d templates per step)" % (per_step, len(bank))
+    elif world > 1:
+        name += " (reference: the first %d of the %d templates per step)" % (len(bank), len(wl.templates))
+    sample = "%d templates of the N=2^22 bank per step over %d processes (scipy float32 rfft for FFTW)" % (
+        per_step, cores)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "bank search, N=2^22, %d templates (sample of %d per step)" % (args.templates, sample),
-                       "n": N, "templates": args.templates},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": "%d templates of the N=2^22 bank per step over %d processes" % (sample, cores)},
+            "config": {"workload": name, "n": N, "templates_per_gpu": args.templates,
+                       "templates_per_step": per_step, "templates": "reference search_parameters (%s)" % kind,
+                       "parallelism": "%d host processes, one template each at a time" % cores},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -332,8 +369,11 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if args.dist_backend == "nccl":
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     import brp_b200 as B
 
     bank = B.Bank([N], [N], count, CAPACITY, device=local)
@@ -345,10 +385,18 @@ def main():
     tarr = B.Bank.params_array(my_templates)
     orbits = np.asarray(wl.orbits[begin:end], np.float64)
     outbuf = np.empty(count * CAPACITY, B.CANDIDATE)
+    all_tarr = B.Bank.params_array(wl.templates) if world > 1 else tarr
+    all_orbits = np.asarray(wl.orbits, np.float64)
 
     def e2e_step():
         bank.set_series(0, x_host)
         return bank.run_flat(tarr, out=outbuf)
+
+    def e2e_fold_step():
+        # the public API end to end: series upload, search of this rank's shard,
+        # candidate lists to the host, bank-wide toplist (gathered to rank 0)
+        bank.set_series(0, x_host)
+        return shard.search_and_fold(bank, tarr, begin, all_tarr, all_orbits, out=outbuf)
 
     # autotune the kernel configuration and templates per launch on this bank
     # (untimed), then warm up through the public API (captures the graph)
@@ -399,18 +447,8 @@ def main():
     # --- end to end through the public API (series H2D + candidates D2H + toplist)
     barrier()
     t0 = time.perf_counter()
-    top = B.Toplist()
-    all_tarr = B.Bank.params_array(wl.templates) if rank == 0 and world > 1 else None
-    all_orbits = np.asarray(wl.orbits, np.float64)
     for _ in range(args.steps):
-        flat, offs, counts, status = e2e_step()
-        if world == 1:
-            top.fold(tarr, orbits, flat, counts)
-        else:
-            # every rank's kept lists to rank 0, folded there in bank order
-            merged = shard.gather_candidates([flat[offs[t]:offs[t + 1]] for t in range(count)], begin)
-            if rank == 0:
-                top.fold(all_tarr, all_orbits, merged)
+        e2e_fold_step()
     torch.cuda.synchronize()
     e2e_ms = 1000 * (time.perf_counter() - t0)
     barrier()
@@ -419,7 +457,8 @@ def main():
     kernel_ms, launches = bank.profile()
 
     if dist:
-        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64,
+                         device="cuda" if args.dist_backend == "nccl" else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_ms, e2e_ms = t.tolist()
 
@@ -436,20 +475,20 @@ def main():
 
     cpu = None
     if pool is not None:
+        # the reference arm's step: the whole bank once over every host core
         cores = host_cores()
-        sample = 64
-        time_cpu(pool, wl.templates, min(cores, sample))
-        secs = time_cpu(pool, wl.templates, sample)
+        time_cpu(pool, wl.templates, cores)
+        secs = time_cpu(pool, wl.templates, count)
         one = time_cpu_one_core(pool, wl.templates)
-        cpu = {"value": sample / secs, "unit": UNIT, "cores": cores, "kind": reference_kind(),
-               "sample": "%d templates of the N=2^22 bank over %d processes (scipy float32 rfft for FFTW)" % (
-                   sample, cores),
+        cpu = {"value": count / secs, "unit": UNIT, "cores": cores, "kind": reference_kind(),
+               "sample": "the whole %d-template N=2^22 bank once over %d processes (scipy float32 rfft for FFTW)"
+                         % (count, cores),
                "one_core_value": 1.0 / one}
-        # parity of this run against the reference's CPU path (untimed); a
-        # failure of the check is reported in the line, not swallowed
+        # parity of this run against the reference's CPU path over the whole
+        # bank (untimed); a failure of the check is reported in the line
         try:
-            accuracy["vs_reference_cpu"] = reference_check(B, bank, pool, my_templates, orbits,
-                                                           min(sample, count), resampled_sha1)
+            accuracy["vs_reference_cpu"] = reference_check(B, bank, pool, my_templates, orbits, count,
+                                                           resampled_sha1)
         except Exception as e:
             accuracy["vs_reference_cpu"] = {"error": "%s: %s" % (type(e).__name__, e)}
         pool.close()
@@ -465,6 +504,8 @@ def main():
     algo = ALGO_BYTES[top_kernel] * N * group
     achieved = algo / (per_launch[top_kernel] * 1e-3) / 1e9
     traffic = measured_traffic().get(top_kernel)
+    traffic_launch = traffic * group if traffic else None
+    achieved_dram = traffic_launch / (per_launch[top_kernel] * 1e-3) / 1e9 if traffic else None
     value = total_templates * args.steps / (dev_ms / 1000)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -480,9 +521,13 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": top_kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic * group if traffic else None,
-                     "algorithmic_bytes_per_launch": algo, "templates_per_launch": group},
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_launch,
+                     "achieved_dram": achieved_dram, "frac_dram": achieved_dram / peak if traffic else None,
+                     "algorithmic_bytes_per_launch": algo, "templates_per_launch": group,
+                     "note": "achieved/frac: algorithmic bytes %dn per template (pass 1 counts its 4n series "
+                             "gather, which the 16 MiB series shared by every template serves from L2); "
+                             "achieved_dram/frac_dram: ncu DRAM bytes of the same launch (profiles/traffic.txt) "
+                             "over its live duration" % ALGO_BYTES[top_kernel]},
         "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": launches,
         "algorithmic_gbs_all_kernels": 16 * N * count / (sum(kernel_ms[k] for k in ALGO_BYTES) * 1e-3) / 1e9,
         "clocks": clock,

@@ -84,7 +84,9 @@ EXPORTS = (
     "brp_toplist_create", "brp_toplist_destroy", "brp_toplist_thresholds", "brp_toplist_retain",
     "brp_toplist_final", "brp_toplist_fold", "brp_cuda_search_static", "brp_cuda_search_static_error",
     "brp_cuda_preprocess", "brp_cuda_preprocess_dd", "brp_cuda_preprocess_error", "brp_host_read_zap",
-    "brp_host_zap_noise", "brp_host_error",
+    "brp_host_zap_noise", "brp_host_error", "brp_cuda_set_wait_limits", "brp_cuda_bank_set_wait_limits",
+    "brp_cuda_debug_fail_allocation", "brp_cuda_bank_autotune", "brp_cuda_load_plan_cache",
+    "brp_cuda_autotune_error",
 )
 
 
@@ -146,6 +148,14 @@ def lib():
             L.brp_toplist_fold.argtypes = [vp, vp, vp, vp, vp, u32]
             L.brp_toplist_final.argtypes = [vp, vp]
             L.brp_toplist_final.restype = u32
+            L.brp_cuda_set_wait_limits.argtypes = [vp, u32, ctypes.c_double]
+            L.brp_cuda_bank_set_wait_limits.argtypes = [vp, u32, ctypes.c_double]
+            L.brp_cuda_debug_fail_allocation.argtypes = [u32]
+            L.brp_cuda_debug_fail_allocation.restype = None
+            L.brp_cuda_bank_autotune.argtypes = [vp, vp, vp, u32, u32, vp, u32, ctypes.c_char_p, u32, vp, u32,
+                                                 ctypes.POINTER(u32)]
+            L.brp_cuda_load_plan_cache.argtypes = [ctypes.c_char_p]
+            L.brp_cuda_autotune_error.restype = ctypes.c_char_p
             _lib = L
     return _lib
 

@@ -86,6 +86,12 @@ class Bank:
         `rows` rows per level (0: all candidates); counts become the kept counts."""
         check(lib().brp_cuda_bank_set_toplist_filter(self._b, rows), self._err)
 
+    def set_wait_limits(self, device_polls=1 << 22, host_seconds=300.0):
+        """Bounds of the run's waits: the host deadline of run()/profile() and
+        the poll bound of a kernel's first wait for its own asynchronous work
+        (0 gives up at once; the template's status then has STATUS_WAIT_TIMEOUT)."""
+        check(lib().brp_cuda_bank_set_wait_limits(self._b, device_polls, host_seconds), self._err)
+
     def launch(self):
         """Replays the last run's graph on the device only (no copies, no wait)."""
         check(lib().brp_cuda_bank_launch(self._b), self._err)

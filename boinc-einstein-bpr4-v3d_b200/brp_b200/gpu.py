@@ -88,6 +88,12 @@ class GPU:
         check(lib().brp_cuda_candidates(self._ctx, slot, ptr(out), n.value, ctypes.byref(n)), self._err)
         return out
 
+    def set_wait_limits(self, device_polls=1 << 22, host_seconds=300.0):
+        """Bounds of run()'s waits (the reference waits without a bound,
+        src/vulkan.cpp:306): the host deadline, and the poll bound of a kernel's
+        first wait for its own asynchronous work (0 gives up at once)."""
+        check(lib().brp_cuda_set_wait_limits(self._ctx, device_polls, host_seconds), self._err)
+
     def device_info(self):
         buf = ctypes.create_string_buffer(1024)
         check(lib().brp_cuda_device_info(self._ctx, buf, len(buf)), self._err)

@@ -38,6 +38,29 @@ def gather_candidates(per_template, begin, group=None):
     return [np.frombuffer(merged[t], dtype=CANDIDATE) for t in sorted(merged)]
 
 
+def search_and_fold(bank, shard_templates, begin, all_templates, all_orbits, out=None, group=None):
+    """One end-to-end step of a rank: searches its template shard
+    (Bank.run_flat; the series is already on the device) and folds the
+    bank-wide toplist of the whole bank in bank order -- directly at world size
+    1, else on rank 0 after gathering every rank's kept candidate lists.
+    `shard_templates` is the rank's Params array (templates begin..), the
+    `all_*` arguments describe the whole bank.  Returns the toplist on rank 0
+    and None elsewhere."""
+    from .host import Toplist
+    flat, offs, counts, status = bank.run_flat(shard_templates, out=out)
+    world, rank = 1, 0
+    try:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            world, rank = dist.get_world_size(group), dist.get_rank(group)
+    except ImportError:
+        pass
+    if world == 1:
+        return Toplist().fold(all_templates, all_orbits, flat, counts)
+    merged = gather_candidates([flat[offs[t]:offs[t + 1]] for t in range(len(counts))], begin, group)
+    return Toplist().fold(all_templates, all_orbits, merged) if rank == 0 else None
+
+
 def fold_toplist(toplist, templates, orbits, candidates):
     """Retains every template's candidates in bank order (src/workunit_main.cpp:124)."""
     if hasattr(toplist, "fold"):

@@ -114,11 +114,14 @@ def config2():
 
 
 def bank_workload(name, lengths, counts, pulsars_per_series, seed, f0=800.0, false_alarm=0.08, window=1000,
-                  sigmas=None, include_truth=True):
+                  sigmas=None, include_truth=True, search=None):
     """Series of the given lengths (no padding: samples = n) with injected
     pulsars, `counts[s]` production templates (src/workload.cpp:108-125) per
     series.  With `sigmas`, templates alternate between per-bin false-alarm
-    levels of those Gaussian sigmas."""
+    levels of those Gaussian sigmas.  `search` computes a template's
+    constants (the signature of search_parameters); by default this package's
+    host code, which is byte-identical to the reference's."""
+    search = search or search_parameters
     rng = np.random.default_rng(seed)
     series, pulsars, templates, series_of, orbits = [], [], [], [], []
     for s, (n, count, npul) in enumerate(zip(lengths, counts, pulsars_per_series)):
@@ -131,7 +134,7 @@ def bank_workload(name, lengths, counts, pulsars_per_series, seed, f0=800.0, fal
                 orb[k * max(1, count // max(1, len(pul)))] = (p.period, p.tau, p.psi)
         for k, (P, tau, psi) in enumerate(orb):
             fa = false_alarm if sigmas is None else sigma_false_alarm(n, sigmas[k % len(sigmas)])
-            templates.append(search_parameters(n, n, SAMPLE_US, P, tau, psi, f0, fa, window))
+            templates.append(search(n, n, SAMPLE_US, P, tau, psi, f0, fa, window))
             series_of.append(s)
             orbits.append((P, tau, psi))
     return Workload(name, series, list(lengths), templates, np.asarray(series_of, np.uint32), orbits, pulsars,

@@ -2,6 +2,7 @@
 // replaces src/vulkan.cpp behind brp::GPU, and the bank extension that runs a
 // whole orbital bank as one captured CUDA graph.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -40,9 +41,23 @@ cudaError_t wait_event(cudaEvent_t ev, double seconds, bool* timed_out) {
     }
 }
 
-constexpr double kWaitSeconds = 300.0;
-
 bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+
+// Host-side fake of a failing cudaMalloc for tests of the error paths
+// (brp_cuda_debug_fail_allocation): when the countdown reaches the allocation
+// it names, that allocation reports failure without calling cudaMalloc.
+std::atomic<uint32_t> g_alloc_countdown{0};
+bool alloc_fault_due() {
+    uint32_t c = g_alloc_countdown.load();
+    while (c)
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    return false;
+}
+
+std::string validate_wait_limits(double seconds) {
+    if (!(seconds >= 0.0) || seconds > 86400.0) return "host deadline must be within 0..86400 seconds";
+    return "";
+}
 
 }  // namespace
 
@@ -64,6 +79,7 @@ struct brp_ctx {
     float* d_power = nullptr;
     double* d_partial = nullptr;
     float* d_mean = nullptr;
+    uint32_t* d_tickets = nullptr;  // pass-1 CTA tickets per template (zero between runs)
     uint32_t* d_status = nullptr;
     uint32_t* d_counts = nullptr;
     brp_candidate* d_cands = nullptr;
@@ -75,6 +91,9 @@ struct brp_ctx {
     std::vector<cudaEvent_t> events;
     uint32_t last_count = 0;
     double last_stage_ms[4] = {0, 0, 0, 0};
+    uint32_t wait_polls = kDefaultWaitPolls;   // device: first-wait poll bound of the kernels
+    double wait_seconds = kDefaultWaitSeconds; // host: deadline of a run
+    cudaEvent_t pending = nullptr;             // completion of a run that passed its deadline
     std::string error;
 
     int fail(int code, const std::string& msg) {
@@ -89,7 +108,7 @@ struct brp_ctx {
     template <class T>
     int alloc(T** p, size_t count, const char* what) {
         size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-        if (cudaMalloc(reinterpret_cast<void**>(p), bytes) != cudaSuccess)
+        if (alloc_fault_due() || cudaMalloc(reinterpret_cast<void**>(p), bytes) != cudaSuccess)
             return fail(BRP_E_RUNTIME, std::string("cudaMalloc failed: ") + what);
         allocations.push_back(*p);
         allocated += bytes;
@@ -186,14 +205,16 @@ extern "C" int brp_cuda_create(const brp_params* params, const float* input, uin
         (st = c->alloc(&c->d_params, B, "params")) || (st = c->alloc(&c->d_work, size_t(slots) * M, "work")) ||
         (st = c->alloc(&c->d_power, size_t(slots) * M, "power")) ||
         (st = c->alloc(&c->d_partial, size_t(slots) * std::max<uint32_t>(c->fused ? c->lp.blocks1() : (p.unpadded + 255) / 256, 1), "partial")) ||
-        (st = c->alloc(&c->d_mean, B, "mean")) || (st = c->alloc(&c->d_status, B, "status")) ||
+        (st = c->alloc(&c->d_mean, B, "mean")) || (st = c->alloc(&c->d_tickets, B, "tickets")) ||
+        (st = c->alloc(&c->d_status, B, "status")) ||
         (st = c->alloc(&c->d_counts, B, "counts")) || (st = c->alloc(&c->d_cands, size_t(B) * cap, "candidates")) ||
         (st = c->alloc(&c->d_raw, p.unpadded, "resampled")) || (st = c->alloc(&c->d_fft, size_t(M) + 1, "fft")) ||
         (st = c->alloc(&c->d_summed, size_t(5) * p.fundamental, "summed")))
         return cleanup(st);
     if (!c->fused && ((st = c->alloc(&c->d_a, M, "fft a")) || (st = c->alloc(&c->d_b, M, "fft b")))) return cleanup(st);
     c->allocated += c->lp.tables_bytes;
-    if ((st = c->cuda(cudaMemcpy(c->d_input, input, size_t(unpadded) * 4, cudaMemcpyHostToDevice), "input upload")))
+    if ((st = c->cuda(cudaMemcpy(c->d_input, input, size_t(unpadded) * 4, cudaMemcpyHostToDevice), "input upload")) ||
+        (st = c->cuda(cudaMemset(c->d_tickets, 0, size_t(B) * 4), "tickets clear")))
         return cleanup(st);
     std::vector<const float*> ptrs(B, c->d_input);
     if ((st = c->cuda(cudaMemcpy(c->d_inputs, ptrs.data(), B * sizeof(void*), cudaMemcpyHostToDevice), "input table")))
@@ -236,17 +257,32 @@ static FusedArgs fused_args(brp_ctx* c, uint32_t count) {
     a.work = c->d_work; a.work_stride = lp.M;
     a.power = c->d_power; a.power_stride = lp.M;
     a.partial = c->d_partial; a.partial_stride = lp.blocks1();
-    a.mean = c->d_mean; a.status = c->d_status; a.counts = c->d_counts; a.cands = c->d_cands;
+    a.mean = c->d_mean; a.tickets = c->d_tickets;
+    a.status = c->d_status; a.counts = c->d_counts; a.cands = c->d_cands;
     a.capacity = c->base.capacity;
     a.snap = int(count) - 1;
     a.snap_raw = c->d_raw; a.snap_fft = c->d_fft; a.snap_summed = c->d_summed;
+    a.wait_polls = c->wait_polls;
     return a;
+}
+
+// A run that passed its host deadline may still be executing: before the next
+// run reuses the context's buffers, wait for it (bounded by the deadline).
+template <class Obj>
+static int settle_pending(Obj* o) {
+    if (!o->pending) return BRP_OK;
+    bool timed_out = false;
+    cudaError_t e = wait_event(o->pending, o->wait_seconds, &timed_out);
+    if (timed_out) return o->fail(BRP_E_TIMEOUT, "the previous run is still executing after the deadline");
+    o->pending = nullptr;
+    return o->cuda(e, "previous run");
 }
 
 extern "C" int brp_cuda_run(brp_ctx* c, brp_timings* timings, double* template_stage_ms) {
     if (!c) return set_thread_error(BRP_E_ARGUMENT, "null context");
     int st;
     if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    if ((st = settle_pending(c))) return st;
     auto start = std::chrono::steady_clock::now();
     double cpu0 = cpu_ms_now();
     const uint32_t count = uint32_t(c->templates.size());
@@ -286,8 +322,11 @@ extern "C" int brp_cuda_run(brp_ctx* c, brp_timings* timings, double* template_s
     double submit_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - submit0).count();
     bool timed_out = false;
     cudaEvent_t done = c->fused ? ev[4] : ev[5 * (count - 1) + 4];
-    cudaError_t e = wait_event(done, kWaitSeconds, &timed_out);
-    if (timed_out) return c->fail(BRP_E_TIMEOUT, "GPU run exceeded its deadline");
+    cudaError_t e = wait_event(done, c->wait_seconds, &timed_out);
+    if (timed_out) {
+        c->pending = done;
+        return c->fail(BRP_E_TIMEOUT, "GPU run exceeded its deadline");
+    }
     if ((st = c->cuda(e, "GPU run"))) return st;
     brp_timings t{};
     t.submit_ms = submit_ms;
@@ -315,7 +354,7 @@ extern "C" int brp_cuda_snapshot(brp_ctx* c, float* resampled, float* fft, float
     if (!c) return set_thread_error(BRP_E_ARGUMENT, "null context");
     if (!c->last_count) return c->fail(BRP_E_RUNTIME, "snapshot before run");
     int st;
-    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) || (st = settle_pending(c))) return st;
     const uint32_t g = c->last_count - 1;
     const brp_params& p = c->templates[g];
     const uint32_t slot = c->fused ? g : 0;
@@ -348,7 +387,7 @@ extern "C" int brp_cuda_candidates(brp_ctx* c, uint32_t slot, brp_candidate* out
     if (slot == UINT32_MAX) slot = c->last_count ? c->last_count - 1 : 0;
     if (slot >= c->last_count) return c->fail(BRP_E_RUNTIME, "candidate slot outside executed batch");
     int st;
-    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice"))) return st;
+    if ((st = c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) || (st = settle_pending(c))) return st;
     uint32_t hdr[2];
     if ((st = c->cuda(cudaMemcpy(&hdr[0], c->d_counts + slot, 4, cudaMemcpyDeviceToHost), "candidates")) ||
         (st = c->cuda(cudaMemcpy(&hdr[1], c->d_status + slot, 4, cudaMemcpyDeviceToHost), "candidates")))
@@ -376,9 +415,10 @@ extern "C" int brp_cuda_device_info(brp_ctx* c, char* buffer, size_t length) {
     cudaDriverGetVersion(&drv);
     snprintf(buffer, length,
              "%s; CUDA sm_%d%d; SMs=%d; runtime=%d; driver=%d; shared_per_block_optin=%zu; L2=%d; pipeline=%s; "
-             "decomposition=%ux%u",
+             "decomposition=%ux%u; pass1=%d; pass2=%d",
              prop.name, prop.major, prop.minor, prop.multiProcessorCount, rt, drv, prop.sharedMemPerBlockOptin,
-             prop.l2CacheSize, c->fused ? "fused" : "plain", c->lp.L1, c->lp.L2);
+             prop.l2CacheSize, c->fused ? "fused" : "plain", c->lp.L1, c->lp.L2, c->lp.fp1 ? c->lp.fp1->id : -1,
+             c->lp.fp2 ? c->lp.fp2->id : -1);
     return BRP_OK;
 }
 
@@ -418,6 +458,7 @@ struct brp_bank {
     const float** d_inputs = nullptr;
     uint32_t *d_counts = nullptr, *d_status = nullptr;
     float* d_mean = nullptr;
+    uint32_t* d_tickets = nullptr;  // pass-1 CTA tickets per template (zero between runs)
     brp_candidate* d_cands = nullptr;
     brp_candidate* d_compact = nullptr;
     uint64_t* d_offsets = nullptr;
@@ -439,6 +480,9 @@ struct brp_bank {
     std::vector<uint32_t> last_sorted_n, last_spans;
     uint32_t last_count = 0;
     cudaEvent_t done = nullptr;
+    uint32_t wait_polls = kDefaultWaitPolls;   // device: first-wait poll bound of the kernels
+    double wait_seconds = kDefaultWaitSeconds; // host: deadline of a run or profile replay
+    cudaEvent_t pending = nullptr;             // completion of a run that passed its deadline
     std::string error;
 
     int fail(int code, const std::string& msg) {
@@ -452,7 +496,8 @@ struct brp_bank {
     }
     template <class T>
     int alloc(T** p, size_t count, const char* what) {
-        if (cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess)
+        if (alloc_fault_due() ||
+            cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess)
             return fail(BRP_E_RUNTIME, std::string("cudaMalloc failed: ") + what);
         allocations.push_back(*p);
         return BRP_OK;
@@ -544,7 +589,13 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
         const LengthPlan& lp = kv.second;
         brp_bank::ClassBuffers cb;
         cb.group = std::min(default_group(lp.n), max_templates);
-        cb.capacity = cb.group;
+        CachedPlan cp;  // a tuned plan of this length: its templates per launch and chains too
+        if (lp.fp1 && lp.fp2 && cached_plan(lp.n, cp) && cp.pass1 == lp.fp1->id && cp.pass2 == lp.fp2->id &&
+            cp.group > 0) {
+            cb.group = std::min(cp.group, max_templates);
+            cb.chains = std::min<uint32_t>(std::max<uint32_t>(cp.chains, 1), 2);
+        }
+        cb.capacity = cb.group * cb.chains;
         cb.partial_per_template = std::max<uint32_t>(lp.blocks1(), lp.M / 64);
         if ((st = b->alloc(&cb.work, size_t(cb.group) * lp.M, "work")) ||
             (st = b->alloc(&cb.power, size_t(cb.group) * lp.M, "power")) ||
@@ -555,7 +606,8 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
     b->compact_cap = uint64_t(max_templates) * capacity;
     if ((st = b->alloc(&b->d_params, max_templates, "params")) || (st = b->alloc(&b->d_inputs, max_templates, "inputs")) ||
         (st = b->alloc(&b->d_counts, max_templates, "counts")) || (st = b->alloc(&b->d_status, max_templates, "status")) ||
-        (st = b->alloc(&b->d_mean, max_templates, "mean")) ||
+        (st = b->alloc(&b->d_mean, max_templates, "mean")) || (st = b->alloc(&b->d_tickets, max_templates, "tickets")) ||
+        (st = b->cuda(cudaMemset(b->d_tickets, 0, size_t(max_templates) * 4), "tickets clear")) ||
         (st = b->alloc(&b->d_cands, size_t(max_templates) * capacity, "candidates")) ||
         (st = b->alloc(&b->d_compact, b->compact_cap, "compact")) ||
         (st = b->alloc(&b->d_offsets, size_t(max_templates) + 1, "offsets")) ||
@@ -632,10 +684,12 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
         a.power = cb.power + size_t(chain) * cb.group * lp.M; a.power_stride = lp.M;
         a.partial = cb.partial + size_t(chain) * cb.group * cb.partial_per_template;
         a.partial_stride = lp.blocks1();
-        a.mean = b->d_mean + t; a.status = b->d_status + t; a.counts = b->d_counts + t;
+        a.mean = b->d_mean + t; a.tickets = b->d_tickets + t;
+        a.status = b->d_status + t; a.counts = b->d_counts + t;
         a.cands = b->d_cands + size_t(t) * b->capacity;
         a.capacity = b->capacity;
         a.snap = -1;
+        a.wait_polls = b->wait_polls;
         uint32_t span = 0;
         for (uint32_t u = t; u < end; ++u) span = std::max(span, spans[u]);
         mark(0, true);
@@ -675,6 +729,9 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     if (!count || count > b->max_templates) return b->fail(BRP_E_ARGUMENT, "template count outside 1..max_templates");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    // The pinned staging buffers below are the sources and targets of the
+    // previous run's copies: a run past its deadline must have finished first.
+    if ((st = settle_pending(b))) return st;
     // Order templates by length class (stable), remembering the caller's order.
     std::vector<uint32_t> order(count);
     for (uint32_t t = 0; t < count; ++t) {
@@ -736,8 +793,11 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     if (b->filter_rows) cudaMemcpyAsync(b->h_kept, b->filter.kept, count * 4, cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b->done, s);
     bool timed_out = false;
-    cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
-    if (timed_out) return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
+    cudaError_t e = wait_event(b->done, b->wait_seconds, &timed_out);
+    if (timed_out) {
+        b->pending = b->done;
+        return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
+    }
     if ((st = b->cuda(e, "bank search"))) return st;
     // The compaction wrote the lists in the caller's order, each sorted by
     // (level, bin); offsets are by caller index.
@@ -813,26 +873,41 @@ extern "C" int brp_cuda_bank_set_toplist_filter(brp_bank* b, uint32_t rows) {
         uint64_t total = 0;
         for (uint32_t s = 0; s < S; ++s) { base[s] = total; half[s] = b->n[s] / 2; total += 5ull * half[s]; }
         if (total >= (1ull << 32)) return b->fail(BRP_E_ARGUMENT, "toplist filter: series too long");
+        // Everything is allocated and initialised into locals first and committed
+        // to the bank only when all of it succeeded, so a failed set-up leaves
+        // the filter off and a later call starts it afresh.
+        FilterArgs f = b->filter;
+        uint32_t* slot_series = nullptr;
         uint64_t* d_base = nullptr;
         uint32_t* d_half = nullptr;
-        if ((st = b->alloc(&b->filter.maxkey, total, "filter")) || (st = b->alloc(&b->filter.flag, total, "filter")) ||
-            (st = b->alloc(&b->filter.owners, total, "filter")) ||
-            (st = b->alloc(&b->filter.owner_count, size_t(S) * 5, "filter")) ||
-            (st = b->alloc(&b->filter.threshold_key, size_t(S) * 5, "filter")) ||
-            (st = b->alloc(&b->filter.kept, b->max_templates, "filter")) ||
-            (st = b->alloc(&b->d_slot_series, b->max_templates, "filter")) || (st = b->alloc(&d_base, S, "filter")) ||
+        uint32_t *h_slot = nullptr, *h_kept = nullptr;
+        if ((st = b->alloc(&f.maxkey, total, "filter")) || (st = b->alloc(&f.flag, total, "filter")) ||
+            (st = b->alloc(&f.owners, total, "filter")) || (st = b->alloc(&f.owner_count, size_t(S) * 5, "filter")) ||
+            (st = b->alloc(&f.threshold_key, size_t(S) * 5, "filter")) ||
+            (st = b->alloc(&f.kept, b->max_templates, "filter")) ||
+            (st = b->alloc(&slot_series, b->max_templates, "filter")) || (st = b->alloc(&d_base, S, "filter")) ||
             (st = b->alloc(&d_half, S, "filter")) ||
-            (st = b->cuda(cudaMemset(b->filter.maxkey, 0, total * 4), "filter clear")) ||
-            (st = b->cuda(cudaMemset(b->filter.flag, 0, total * 4), "filter clear")) ||
-            (st = b->cuda(cudaMemset(b->filter.owner_count, 0, size_t(S) * 5 * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemset(f.maxkey, 0, total * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemset(f.flag, 0, total * 4), "filter clear")) ||
+            (st = b->cuda(cudaMemset(f.owner_count, 0, size_t(S) * 5 * 4), "filter clear")) ||
             (st = b->cuda(cudaMemcpy(d_base, base.data(), S * 8, cudaMemcpyHostToDevice), "filter upload")) ||
             (st = b->cuda(cudaMemcpy(d_half, half.data(), S * 4, cudaMemcpyHostToDevice), "filter upload")) ||
-            (st = b->cuda(cudaMallocHost(&b->h_slot_series, b->max_templates * sizeof(uint32_t)), "cudaMallocHost")) ||
-            (st = b->cuda(cudaMallocHost(&b->h_kept, b->max_templates * sizeof(uint32_t)), "cudaMallocHost")))
+            (st = b->cuda(cudaMallocHost(&h_slot, b->max_templates * sizeof(uint32_t)), "cudaMallocHost")) ||
+            (st = b->cuda(cudaMallocHost(&h_kept, b->max_templates * sizeof(uint32_t)), "cudaMallocHost"))) {
+            for (void* p : {(void*)f.maxkey, (void*)f.flag, (void*)f.owners, (void*)f.owner_count,
+                            (void*)f.threshold_key, (void*)f.kept, (void*)slot_series, (void*)d_base, (void*)d_half})
+                if (p) b->release(p);
+            if (h_slot) cudaFreeHost(h_slot);
+            if (h_kept) cudaFreeHost(h_kept);
             return st;
-        b->filter.base = d_base;
-        b->filter.half = d_half;
-        b->filter.series = S;
+        }
+        f.base = d_base;
+        f.half = d_half;
+        f.series = S;
+        b->filter = f;
+        b->d_slot_series = slot_series;
+        b->h_slot_series = h_slot;
+        b->h_kept = h_kept;
     }
     b->filter_rows = rows;
     b->filter.rows = rows;
@@ -864,13 +939,17 @@ extern "C" int brp_cuda_bank_profile(brp_bank* b, double* kernel_ms, uint32_t* l
     if (!b || !kernel_ms) return set_thread_error(BRP_E_ARGUMENT, "null argument");
     if (!b->last_count) return b->fail(BRP_E_ARGUMENT, "no bank run to profile");
     int st;
-    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) || (st = settle_pending(b))) return st;
     KernelEvents prof;
     record_bank(b, b->last_sorted_n, b->last_spans, b->last_count, &prof);
     cudaEventRecord(b->done, b->stream);
     bool timed_out = false;
-    cudaError_t e = wait_event(b->done, kWaitSeconds, &timed_out);
-    if (timed_out) return b->fail(BRP_E_TIMEOUT, "bank profile exceeded its deadline");
+    cudaError_t e = wait_event(b->done, b->wait_seconds, &timed_out);
+    if (timed_out) {
+        b->pending = b->done;
+        for (auto ev : prof.ev) cudaEventDestroy(ev);  // released once the replay reaches them
+        return b->fail(BRP_E_TIMEOUT, "bank profile exceeded its deadline");
+    }
     if ((st = b->cuda(e, "bank profile"))) return st;
     for (int k = 0; k < 4; ++k) { kernel_ms[k] = 0; if (launches) launches[k] = 0; }
     for (size_t i = 0; i < prof.kind.size(); ++i) {
@@ -885,3 +964,34 @@ extern "C" int brp_cuda_bank_profile(brp_bank* b, double* kernel_ms, uint32_t* l
 
 extern "C" void* brp_cuda_bank_stream(brp_bank* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
 extern "C" uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* b) { return b ? b->kernels_per_run : 0; }
+
+// ============================================================ wait limits
+template <class Obj>
+static int set_wait_limits(Obj* o, uint32_t device_polls, double host_seconds) {
+    std::string v = validate_wait_limits(host_seconds);
+    if (!v.empty()) return o->fail(BRP_E_ARGUMENT, v);
+    o->wait_polls = device_polls;
+    o->wait_seconds = host_seconds;
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_set_wait_limits(brp_ctx* c, uint32_t device_polls, double host_seconds) {
+    if (!c) return set_thread_error(BRP_E_ARGUMENT, "null context");
+    return set_wait_limits(c, device_polls, host_seconds);
+}
+
+extern "C" int brp_cuda_bank_set_wait_limits(brp_bank* b, uint32_t device_polls, double host_seconds) {
+    if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    const uint32_t before = b->wait_polls;
+    int st = set_wait_limits(b, device_polls, host_seconds);
+    if (!st && before != device_polls) {
+        // the poll bound is a launch argument of the captured kernels
+        if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) ||
+            (st = b->cuda(cudaStreamSynchronize(b->stream), "wait limits")))
+            return st;
+        b->drop_graph();
+    }
+    return st;
+}
+
+extern "C" void brp_cuda_debug_fail_allocation(uint32_t after) { g_alloc_countdown.store(after); }

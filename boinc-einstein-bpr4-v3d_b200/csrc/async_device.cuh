@@ -26,10 +26,15 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
+// Poll bound of a wait that must end before a CTA may leave (its own bulk
+// copies or MMAs still write its shared or tensor memory): far above any copy
+// or MMA latency (at least ~0.5 s with the back-off below).
+constexpr uint32_t kDrainPolls = 1u << 22;
+
 // Waits for the phase of the given parity to complete; gives up (returns
-// false) after about 2^22 polls, a bound far above any copy or MMA latency.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 22); ++it) {
+// false) after `polls` polls (0: at once, without polling).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint32_t polls = kDrainPolls) {
+    for (uint32_t it = 0; it < polls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

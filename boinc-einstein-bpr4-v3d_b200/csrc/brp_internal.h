@@ -50,11 +50,15 @@ struct LengthPlan {
 // error message or empty.  fast1/fast2 (optional) force compiled pass
 // configurations by id (0: default choice, -1: generic kernels).
 std::string make_length_plan(uint32_t n, LengthPlan& plan, cudaStream_t stream, int fast1 = 0, int fast2 = 0);
+// The tuned plan of length n for the current device from the plan cache
+// (autotune.cu): the entry tuned on the largest bank of that length.
+struct CachedPlan { int pass1 = 0, pass2 = 0; uint32_t group = 0, chains = 1; };
+bool cached_plan(uint32_t n, CachedPlan& out);
 // The parts of make_length_plan: the decomposition and kernel choice (no
 // allocation), the table layout (offsets[12], returns the float2 count;
 // with_plain adds the table of the step-by-step pipeline) and the table fill
 // (host[] laid out by the layout, lp's views pointed at dev).
-std::string choose_length_plan(uint32_t n, LengthPlan& plan, int fast1 = 0, int fast2 = 0);
+std::string choose_length_plan(uint32_t n, LengthPlan& plan, int fast1 = 0, int fast2 = 0, bool use_cache = true);
 size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t offsets[12]);
 void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, float2* dev);
 void free_length_plan(LengthPlan& plan);
@@ -81,6 +85,7 @@ struct FastPass {
 // tensor-core form, fused_tc.cu) follow the CUDA-core ones and are chosen only
 // by id.
 const std::vector<FastPass>& fast_pass1_configs();
+void append_pass1_warp_configs(std::vector<FastPass>& v);
 void append_pass1_tc_configs(std::vector<FastPass>& v);
 const std::vector<FastPass>& fast_pass2_configs();
 size_t harmonic_fast_smem();
@@ -100,7 +105,8 @@ struct FusedArgs {
     size_t power_stride;
     double* partial;  // per template: blocks1 partial sums of the resampled series
     uint32_t partial_stride;
-    float* mean;      // per template: padding value (written by pass 2)
+    float* mean;      // per template: padding value (compiled kernels: pass 1's last CTA; generic: pass 2)
+    uint32_t* tickets;  // per template: pass-1 CTAs done (compiled kernels; zero between launches)
     uint32_t* status; // per template: BRP_STATUS_* bits
     uint32_t* counts; // per template: candidate count
     brp_candidate* cands;  // per template: capacity candidates
@@ -110,7 +116,16 @@ struct FusedArgs {
     float* snap_raw;     // resampled series (first steps values)
     float2* snap_fft;    // X[0..M]
     float* snap_summed;  // 5*fundamental
+    // Poll bound of a kernel's first wait for its own asynchronous work (the
+    // harmonic kernel's staging copies, the tensor-core pass 1's MMAs); on
+    // expiry the template's status gets BRP_STATUS_WAIT_TIMEOUT and the kernel
+    // drains that work with the full bound before the CTA leaves.
+    uint32_t wait_polls;
 };
+// Default of FusedArgs::wait_polls and of the per-context / per-bank device
+// wait limit; default host deadline of a run (seconds).
+constexpr uint32_t kDefaultWaitPolls = 1u << 22;
+constexpr double kDefaultWaitSeconds = 300.0;
 
 cudaError_t set_fused_attributes(size_t max_dynamic_smem);
 void launch_fused_pass1(const FusedArgs& a, const LengthPlan& lp, uint32_t count, cudaStream_t s);

@@ -9,7 +9,7 @@ TMP=$(mktemp -d)
 trap 'rm -rf "$TMP"' EXIT
 FLAGS="-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 -Xcompiler -fPIC,-ffp-contract=off"
 PIDS=""
-for f in api plan fused_kernels fused_fast fused_tc harmonic_fast plain_kernels static_search toplist_filter whiten; do
+for f in api autotune plan fused_kernels fused_fast fused_tc harmonic_fast pass1_warp plain_kernels static_search toplist_filter whiten; do
   $NVCC $FLAGS -c "$HERE/$f.cu" -o "$TMP/$f.o" &
   PIDS="$PIDS $!"
 done

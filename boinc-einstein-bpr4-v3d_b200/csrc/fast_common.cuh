@@ -20,7 +20,14 @@
 namespace brp {
 namespace {
 
-__constant__ uint32_t c_fast_lut_bits[130] = BRP_LUT_BITS;
+// (sine, cosine) bit pairs: entry li is read as one 64-bit constant load
+__constant__ __align__(8) uint32_t c_fast_lut_bits[130] = BRP_LUT_BITS;
+
+// Gather modes: the low two bits select the index arithmetic (0: FP32
+// reference order, 1: FP32 with the reference's FMA forms, 2: FP64 time
+// index); kSmallIndex adds that every sample index is below 2^23, so float(i)
+// needs no fallback for larger indices.
+constexpr int kSmallIndex = 4;
 
 // Shared-memory layout of the compiled kernels: element e of a sequence at
 // e + e / 16 (one padding slot per 16 keeps radix-16 strided stores on distinct
@@ -100,13 +107,15 @@ __host__ __device__ constexpr int ct_table_size() {
 }
 
 // ---- bit-identical lean resampling index (see the file comment) ----
+template <bool SMALL>
 __device__ __forceinline__ float u2f_exact(uint32_t i) {
+    if (SMALL) return __fsub_rn(__int_as_float(0x4B000000 | int(i)), 8388608.0f);  // i < 2^23
     return i < (1u << 23) ? __fsub_rn(__int_as_float(0x4B000000 | int(i)), 8388608.0f) : __uint2float_rn(i);
 }
 
-template <bool FMA>
+template <bool FMA, bool SMALL = false>
 __device__ __forceinline__ int lean_index(uint32_t i, const brp_resample_consts& p) {
-    const float fi = u2f_exact(i);
+    const float fi = u2f_exact<SMALL>(i);
     const float t = __fmul_rn(fi, p.dt);
     const float ph = FMA ? __fmaf_rn(p.omega, t, p.psi) : __fadd_rn(__fmul_rn(p.omega, t), p.psi);
     const float y = __fmul_rn(BRP_INV_TWO_PI_F, ph);
@@ -116,7 +125,8 @@ __device__ __forceinline__ int lean_index(uint32_t i, const brp_resample_consts&
     const float mg = __fadd_rd(x64, 8388608.0f);
     const int li = __float_as_int(mg) - 0x4B000000;
     const float fli = __fsub_rn(mg, 8388608.0f);
-    const float s = __uint_as_float(c_fast_lut_bits[2 * li]), c = __uint_as_float(c_fast_lut_bits[2 * li + 1]);
+    const uint2 sc = reinterpret_cast<const uint2*>(c_fast_lut_bits)[li];
+    const float s = __uint_as_float(sc.x), c = __uint_as_float(sc.y);
     float sn, off;
     if (FMA) {
         const float d = __fmul_rn(BRP_TWO_PI_F, __fmaf_rn(-fli, 0.015625f, xt));
@@ -156,6 +166,34 @@ __device__ __forceinline__ double block_sum_d(double v, double* scratch) {
     return r;
 }
 
+// Publishes this pass-1 CTA's FP64 sum of its samples (tot, valid in thread 0)
+// and, in the CTA that completes the template's set (an atomic ticket taken
+// after a fence), the template's padding value a.mean[g] = sum / steps, the
+// partials summed in a fixed order.  That CTA re-arms the ticket, so the
+// counters are zero again after every launch.  Every thread of the CTA calls
+// this; it synchronises the CTA.
+template <int THREADS>
+__device__ __forceinline__ void publish_mean(const FusedArgs& a, int g, uint32_t steps, double tot, double* red) {
+    __shared__ int s_last;
+    double* pp = a.partial + size_t(g) * a.partial_stride;
+    if (threadIdx.x == 0) {
+        pp[blockIdx.x] = tot;
+        __threadfence();
+        s_last = atomicAdd(a.tickets + g, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double part = 0;
+        for (uint32_t i = threadIdx.x; i < gridDim.x; i += THREADS) part += __ldcg(pp + i);
+        const double all = block_sum_d<THREADS>(part, red);
+        if (threadIdx.x == 0) {
+            a.mean[g] = float(all / double(steps));
+            a.tickets[g] = 0;
+        }
+    }
+}
+
 // Gathers this CTA's samples (rows n1 < L1, C complex points = 2C consecutive
 // reals per row) into shared memory; returns the sum of the samples (FP32 per
 // thread, a few dozen samples, then FP64 across threads).  Thread t handles
@@ -189,8 +227,8 @@ __device__ __forceinline__ double gather(float2* sm, const float* __restrict__ i
             j[b] = -1;
             if (ib < steps) {
                 int jj;
-                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<MODE == 1>(ib, rc);
+                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
+                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
                 if (uint32_t(jj) < unpadded) j[b] = jj;
                 else oob = true;
             }
@@ -243,8 +281,8 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
             jx[b] = -1;
             if (ib < steps) {
                 int jj;
-                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<MODE == 1>(ib, rc);
+                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
+                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
                 if (uint32_t(jj) < unpadded) jx[b] = jj;
                 else oob = true;
             }

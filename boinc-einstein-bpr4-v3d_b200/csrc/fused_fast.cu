@@ -26,19 +26,23 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     float* raw = (g == a.snap) ? a.snap_raw : nullptr;
     bool oob = false;
     double sum;
+    const bool small = P.unpadded <= (1u << 23);  // every sample index below 2^23
     if constexpr (FIRST) {
+        constexpr int S = kSmallIndex;
         if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather_dft16<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
+        else if ((P.flags & 2u) && small) sum = gather_dft16<L1, C, THREADS, STRIDE, 1 | S>(sm, in, P, L2, c0, raw, oob);
         else if (P.flags & 2u) sum = gather_dft16<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
+        else if (small) sum = gather_dft16<L1, C, THREADS, STRIDE, S>(sm, in, P, L2, c0, raw, oob);
         else sum = gather_dft16<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
     } else {
         if (P.flags & BRP_FLAG_INDEX_FP64) sum = gather<L1, C, THREADS, STRIDE, 2>(sm, in, P, L2, c0, raw, oob);
+        else if ((P.flags & 2u) && small) sum = gather<L1, C, THREADS, STRIDE, 1 | kSmallIndex>(sm, in, P, L2, c0, raw, oob);
         else if (P.flags & 2u) sum = gather<L1, C, THREADS, STRIDE, 1>(sm, in, P, L2, c0, raw, oob);
         else sum = gather<L1, C, THREADS, STRIDE, 0>(sm, in, P, L2, c0, raw, oob);
     }
     if (oob) atomicOr(a.status + g, BRP_STATUS_RESAMPLE_OOB);
     const double tot = block_sum_d<THREADS>(sum, red);
-    if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
-    __syncthreads();
+    publish_mean<THREADS>(a, g, P.steps, tot, red);
 
     float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
     if constexpr (FIRST) ct_fft_store<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
@@ -144,8 +148,6 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     // first pass (radix 16) fused into the row loads when each thread owns one of its butterflies
     constexpr bool FIRST = R0 == 16 && SEQ * L2 == 16 * THREADS;
     extern __shared__ __align__(16) float2 sm[];
-    __shared__ double red[THREADS / 32];
-    __shared__ float s_mean;
     const int g = blockIdx.y, q = blockIdx.x;
     const brp_params& P = a.params[g];
     const uint32_t L1 = a.L1, n = a.n, M = a.M, steps = P.steps;
@@ -172,17 +174,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             sm[rr * STRIDE + ct_pos(k2 + 1)] = make_float2(x.z, x.w);
         }
     }
-    double part = 0;
-    const double* pp = a.partial + size_t(g) * a.partial_stride;
-    for (uint32_t i = threadIdx.x; i < a.partial_stride; i += THREADS) part += pp[i];
-    const double tot = block_sum_d<THREADS>(part, red);
-    if (threadIdx.x == 0) {
-        const float mean = float(tot / double(steps));
-        s_mean = mean;
-        if (q == 0) a.mean[g] = mean;
-    }
-    __syncthreads();
-    const float mean = s_mean;
+    const float mean = __ldg(a.mean + g);  // published by pass 1's last CTA of the template
+    __syncthreads();  // the row loads in shared memory before the next pass reads them
 
     float* __restrict__ Pw = a.power + size_t(g) * a.power_stride;
     float2* fft = (g == a.snap) ? a.snap_fft : nullptr;
@@ -321,6 +314,7 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<1536, 2, 192, 5, 16, 4, 3, 8>::info(122),
         P1<2048, 8, 1024, 1, 16, 8, 16>::info(123),
     };
+    append_pass1_warp_configs(v);
     append_pass1_tc_configs(v);
     return v;
 }

@@ -405,6 +405,7 @@ void fill_fused_args(FusedArgs& a, const LengthPlan& lp) {
     a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
     a.ptw1 = lp.ptw1; a.ptw2 = lp.ptw2;
     a.hf_hi = lp.hf_hi; a.hf_lo = lp.hf_lo;
+    a.wait_polls = kDefaultWaitPolls;
 }
 
 }  // namespace brp

@@ -132,8 +132,8 @@ __device__ __forceinline__ double gather_rows(unsigned char* A, const float* __r
             jx[b] = -1;
             if (ib < steps) {
                 int jj;
-                if (MODE == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<MODE == 1>(ib, rc);
+                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
+                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
                 if (uint32_t(jj) < unpadded) jx[b] = jj;
                 else oob = true;
             }
@@ -233,8 +233,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     const double tot = block_sum_d<THREADS>(sum, red);  // synchronises the CTA
-    if (threadIdx.x == 0) a.partial[size_t(g) * a.partial_stride + blockIdx.x] = tot;
-    __syncthreads();
+    publish_mean<THREADS>(a, g, P.steps, tot, red);      // before any early exit below
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
@@ -257,8 +256,11 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_tc(FusedArgs a) {
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                      : "memory");
     }
-    const bool done = mbar_wait_bounded(bar, 0);
+    const bool done = mbar_wait_bounded(bar, 0, a.wait_polls);
     const int timed_out = __syncthreads_or(!done);
+    // On expiry the MMAs may still write this CTA's tensor memory and read its
+    // operand tiles: drain them (full bound) before the memory is freed.
+    if (timed_out) mbar_wait_bounded(bar, 0, kDrainPolls);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!timed_out && warp < 4 * TILES) {
         const int quad = warp & 3, tile = warp >> 2;

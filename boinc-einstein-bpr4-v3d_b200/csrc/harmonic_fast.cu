@@ -127,8 +127,21 @@ __device__ __forceinline__ void level_local(const float (&v)[16], uint32_t i0, b
                                             brp_candidate* out, uint32_t capacity, uint32_t* status,
                                             LevelTail& head, LevelTail& tail) {
     constexpr int W = 1 << H, HALF = W / 2;
+    // Without a summed-array snapshot only candidates matter, and a fundamental
+    // bin is one only if its value exceeds thr: the largest sum when that exceeds
+    // thr (the first sum never does then), else 0 for an empty range (only
+    // when thr < 0).  So one maximum over the trial bins of the local
+    // fundamentals [HALF, 16 - HALF) decides whether any of them needs a look.
+    bool detail = true;
+    if (16 / W > 1 && !summed) {
+        float lm = v[HALF];
+#pragma unroll
+        for (int r = HALF + 1; r < 16 - HALF; ++r) lm = fmaxf(lm, v[r]);
+        detail = lm > thr || (!ALLV && thr < 0.f);
+    }
 #pragma unroll
     for (int u = 1; u < 16 / W; ++u) {
+        if (!detail) break;
         float best, first;
         if (ALLV) {
             first = v[u * W - HALF];
@@ -192,29 +205,35 @@ struct HCtx {
     uint32_t* status;
 };
 
+// Masks the sums of the thread's trial bins for level bookkeeping: outside
+// [window, harmonic) (and before bin 0) a bin takes the -1 sentinel.
 template <bool ALLV>
-__device__ __forceinline__ void sums_and_levels(const HCtx& c, const float (&p16)[16], LevelTail (&head)[4],
-                                                LevelTail (&tail)[4]) {
-    float s[16], t[16], v[16];
-    auto mask = [&]() {
+__device__ __forceinline__ void masked(const HCtx& c, const float (&s)[16], float (&v)[16]) {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-            if (ALLV) v[r] = s[r];
-            else {
-                const int64_t i = c.mp * 16 + r;
-                v[r] = (c.mp >= 0 && i >= int64_t(c.window) && i < int64_t(c.harmonic)) ? s[r] : -1.f;
-            }
+    for (int r = 0; r < 16; ++r) {
+        if (ALLV) v[r] = s[r];
+        else {
+            const int64_t i = c.mp * 16 + r;
+            v[r] = (c.mp >= 0 && i >= int64_t(c.window) && i < int64_t(c.harmonic)) ? s[r] : -1.f;
         }
-    };
+    }
+}
+
+// Levels 1-3 (stages A-C): the even factors, read straight from global memory,
+// so they run while the odd factors' staging copies are still in flight.
+// Leaves s = s8 for stage D.
+template <bool ALLV>
+__device__ __forceinline__ void sums_abc(const HCtx& c, const float (&p16)[16], float (&s)[16], LevelTail (&head)[4],
+                                         LevelTail (&tail)[4]) {
+    float t[16], v[16];
     float* sm1 = c.summed ? c.summed + size_t(c.fundamental) : nullptr;
     float* sm2 = c.summed ? c.summed + size_t(2) * c.fundamental : nullptr;
     float* sm3 = c.summed ? c.summed + size_t(3) * c.fundamental : nullptr;
-    float* sm4 = c.summed ? c.summed + size_t(4) * c.fundamental : nullptr;
     // stage A: s2 = P16 + P8 (P16 = the level-0 values)
 #pragma unroll
     for (int r = 0; r < 16; ++r) s[r] = p16[r];
     add_factor<8, false>(s, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
-    mask();
+    masked<ALLV>(c, s, v);
     level_local<1, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[1], sm1, c.count, c.out, c.cap, c.status,
                          head[0], tail[0]);
     // stage B: s4 = s2 + (P12 + P4)
@@ -222,7 +241,7 @@ __device__ __forceinline__ void sums_and_levels(const HCtx& c, const float (&p16
     add_factor<4, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
 #pragma unroll
     for (int r = 0; r < 16; ++r) s[r] += t[r];
-    mask();
+    masked<ALLV>(c, s, v);
     level_local<2, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[2], sm2, c.count, c.out, c.cap, c.status,
                          head[1], tail[1]);
     // stage C: s8 = s4 + (((P14 + P10) + P6) + P2)
@@ -232,10 +251,17 @@ __device__ __forceinline__ void sums_and_levels(const HCtx& c, const float (&p16
     add_factor<2, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
 #pragma unroll
     for (int r = 0; r < 16; ++r) s[r] += t[r];
-    mask();
+    masked<ALLV>(c, s, v);
     level_local<3, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[3], sm3, c.count, c.out, c.cap, c.status,
                          head[2], tail[2]);
-    // stage D: s16 = s8 + (((((((P15 + P13) + P11) + P9) + P7) + P5) + P3) + P1)
+}
+
+// Level 4 (stage D): s16 = s8 + (((((((P15 + P13) + P11) + P9) + P7) + P5) + P3) + P1)
+// from the odd factors staged in shared memory.
+template <bool ALLV>
+__device__ __forceinline__ void sums_d(const HCtx& c, float (&s)[16], LevelTail& head, LevelTail& tail) {
+    float t[16], v[16];
+    float* sm4 = c.summed ? c.summed + size_t(4) * c.fundamental : nullptr;
     add_factor<15, true>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<13, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<11, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
@@ -246,9 +272,9 @@ __device__ __forceinline__ void sums_and_levels(const HCtx& c, const float (&p16
     add_factor<1, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
 #pragma unroll
     for (int r = 0; r < 16; ++r) s[r] += t[r];
-    mask();
+    masked<ALLV>(c, s, v);
     level_local<4, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[4], sm4, c.count, c.out, c.cap, c.status,
-                         head[3], tail[3]);
+                         head, tail);
 }
 
 // Six CTAs per SM (80 registers per thread): the shared-memory staging allows
@@ -272,11 +298,11 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     // ---- stage the odd factors.  Interior CTAs (every region inside [0, M)):
     // one bulk copy per region, issued by thread 0 and counted on an mbarrier.
     // Edge CTAs: 16-byte asynchronous copies from a 16-byte aligned start,
-    // chunks reaching outside [0, M) copied element-wise with zero fill.
+    // chunks reaching outside [0, M) copied element-wise with zero fill.  The
+    // copies are only waited for before stage D, the first to read them.
     const uint32_t stage_sh = smem_u32(stage);
     const uint32_t bar = smem_u32(&s_bar);
     const bool bulk = first >= 0 && ((first * 15) & ~int64_t(3)) + region_floats(15) <= int64_t(M);
-    bool copied = true;
     if (bulk) {
         if (threadIdx.x == 0) {
             mbar_init(bar, 1);
@@ -289,7 +315,6 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
             }
         }
         __syncthreads();  // the barrier is initialised before anyone polls it
-        copied = mbar_wait_bounded(bar, 0);
     } else {
 #pragma unroll 1
         for (int k = 1; k <= 15; k += 2) {
@@ -314,14 +339,7 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
                 }
             }
         }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-    }
-    if (__syncthreads_or(!copied)) {
-        // A bulk copy did not complete within the bound: report it, give the
-        // copies one more bounded wait (they write this CTA's shared memory) and leave.
-        if (threadIdx.x == 0) atomicOr(a.status + g, BRP_STATUS_WAIT_TIMEOUT);
-        mbar_wait_bounded(bar, 0);
-        return;
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
 
     HCtx c;
@@ -352,7 +370,16 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
             p0[r] = (gi >= 0 && gi < int64_t(M)) ? __ldg(Pw + gi) : 0.f;
         }
     }
-    if (c.own) {
+    // level 0: only bins above threshold[0] are candidates, so without a
+    // summed-array snapshot one maximum decides whether the bins need a look
+    bool look = c.own;
+    if (look && !summed) {
+        float mx = p0[0];
+#pragma unroll
+        for (int r = 1; r < 16; ++r) mx = fmaxf(mx, p0[r]);
+        look = mx > P.threshold[0];
+    }
+    if (look) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
             const uint32_t j = c.i0 + r;
@@ -364,8 +391,23 @@ __global__ void __launch_bounds__(kHThreads, 6) harmonic_fast_kernel(FusedArgs a
     }
 
     LevelTail head[4], tail[4];
-    if (all_valid) sums_and_levels<true>(c, p0, head, tail);
-    else sums_and_levels<false>(c, p0, head, tail);
+    float s8[16];
+    if (all_valid) sums_abc<true>(c, p0, s8, head, tail);
+    else sums_abc<false>(c, p0, s8, head, tail);
+
+    // the odd factors' staging must have landed before stage D
+    bool copied = true;
+    if (bulk) copied = mbar_wait_bounded(bar, 0, a.wait_polls);
+    else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (__syncthreads_or(!copied)) {
+        // A bulk copy did not complete within the bound: report it, give the
+        // copies one more bounded wait (they write this CTA's shared memory) and leave.
+        if (threadIdx.x == 0) atomicOr(a.status + g, BRP_STATUS_WAIT_TIMEOUT);
+        mbar_wait_bounded(bar, 0, kDrainPolls);
+        return;
+    }
+    if (all_valid) sums_d<true>(c, s8, head[3], tail[3]);
+    else sums_d<false>(c, s8, head[3], tail[3]);
 
     // ---- u = 0 fundamental bins: previous thread's tail + own head
     const int lane = m & 31, warp = m >> 5;

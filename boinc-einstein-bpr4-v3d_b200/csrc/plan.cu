@@ -66,9 +66,10 @@ static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
     }
 }
 
-// The compiled pass pair a length takes when the caller names none: the pairs
-// the autotuner chose on one B200 for bank workloads of these lengths (n = 2^20,
-// 3*2^20, 2^22, 3*2^21).  Other lengths take the first compiled pair that fits.
+// The compiled pass pair a length takes when the caller names none and the
+// plan cache has no tuned plan for it: the pairs the autotuner chose on one
+// B200 for bank workloads of these lengths (n = 2^20, 3*2^20, 2^22, 3*2^21).
+// Other lengths take the first compiled pair that fits.
 static void preferred_pair(uint32_t M, int& id1, int& id2) {
     id1 = id2 = 0;
     if (M == (1u << 19)) { id1 = 120; id2 = 202; }
@@ -77,7 +78,7 @@ static void preferred_pair(uint32_t M, int& id1, int& id2) {
     if (M == (3u << 20)) { id1 = 119; id2 = 204; }
 }
 
-std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2) {
+std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2, bool use_cache) {
     const bool radix3 = !is_pow2(n);
     if (n < 64 || n > 3u * (1u << 22) || (radix3 && !(n % 3 == 0 && is_pow2(n / 3))))
         return "series length must be 2^k or 3*2^k in 64..3*2^22";
@@ -92,7 +93,12 @@ std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2)
     // Compiled two-pass decomposition when one exists (rows of 1024 preferred).
     if (lp.M >= 4096 && fast1 >= 0 && fast2 >= 0) {
         int want1[2] = {fast1, fast1}, want2[2] = {fast2, fast2};
-        if (!fast1 && !fast2) preferred_pair(lp.M, want1[0], want2[0]);
+        CachedPlan cp;
+        if (!fast1 && !fast2) {
+            // the autotuner's plan for this length and device, else the pairs it chose on one B200
+            if (use_cache && cached_plan(n, cp)) { want1[0] = cp.pass1; want2[0] = cp.pass2; }
+            else preferred_pair(lp.M, want1[0], want2[0]);
+        }
         for (int attempt = 0; attempt < 2 && !lp.fp1; ++attempt)
             for (uint32_t l2 : {1024u, 512u, 2048u, 256u}) {
                 if (lp.M % l2 || lp.M / l2 > 4096) continue;

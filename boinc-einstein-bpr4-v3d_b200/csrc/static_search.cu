@@ -12,7 +12,16 @@
 // The array is part of the module: every GPU that loads the library holds it
 // (kScratchBytes, about 4.2 MiB) until the process exits.  Host code only sees
 // a stand-in for it; its device address comes from cudaGetSymbolAddress, once
-// per device, with that device current.
+// per device, with that device current.  The cached address and the tables
+// copied into the array belong to the device's context: after a
+// cudaDeviceReset in the same process the entry point must not be called
+// again on that device.
+//
+// Per call, the template constants and the series pointer reach the array
+// through one single-thread kernel that takes them by value (no host staging
+// buffer), so a call after set-up only enqueues kernels on the caller's
+// stream and returns.
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include "brp_internal.h"
@@ -27,7 +36,7 @@ constexpr size_t kTableEntries = 16384;                                  // twid
 constexpr size_t kTableBytes = kTableEntries * sizeof(float2);
 constexpr uint32_t kMaxPartials = 4096;                                  // pass-1 CTAs of one template
 constexpr size_t kPartialBytes = kMaxPartials * sizeof(double);
-constexpr size_t kMiscBytes = 512;  // brp_params, the input pointer, the padding value
+constexpr size_t kMiscBytes = 512;  // brp_params, the input pointer, the padding value, the pass-1 ticket
 constexpr size_t kScratchBytes = kWorkBytes + kTableBytes + kPartialBytes + kMiscBytes;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -49,6 +58,18 @@ int static_fail(int code, const char* msg) {
     return code;
 }
 
+// Writes one call's arguments into the array and clears the caller's count
+// and status words.
+__global__ void static_args_kernel(brp_params p, const float* input, brp_params* d_params, const float** d_input,
+                                   uint32_t* count, uint32_t* status) {
+    *d_params = p;
+    *d_input = input;
+    *count = 0;
+    *status = 0;
+}
+
+bool misaligned(const void* ptr, uintptr_t bytes) { return (reinterpret_cast<uintptr_t>(ptr) & (bytes - 1)) != 0; }
+
 }  // namespace
 }  // namespace brp
 
@@ -61,6 +82,13 @@ extern "C" int brp_cuda_search_static(const brp_params* params, const float* inp
                                       uint32_t* status, void* stream) {
     if (!params || !input || !power || !candidates || !count || !status || !capacity)
         return static_fail(BRP_E_ARGUMENT, "null buffer or zero capacity");
+    // The harmonic kernel stages the power spectrum with 16-byte bulk and
+    // vector copies; candidates are 16-byte records; the series, the count and
+    // the status word are read and updated as 32-bit words.
+    if (misaligned(power, 16) || misaligned(candidates, 16))
+        return static_fail(BRP_E_ARGUMENT, "power and candidates must be 16-byte aligned");
+    if (misaligned(input, 4) || misaligned(count, 4) || misaligned(status, 4))
+        return static_fail(BRP_E_ARGUMENT, "input, count and status must be 4-byte aligned");
     const brp_params& p = *params;
     const bool pow2 = p.n && !(p.n & (p.n - 1));
     if (!(pow2 || (p.n % 3 == 0 && !((p.n / 3) & (p.n / 3 - 1)))))
@@ -91,12 +119,14 @@ extern "C" int brp_cuda_search_static(const brp_params* params, const float* inp
     brp_params* d_params = reinterpret_cast<brp_params*>(misc);
     const float** d_input = reinterpret_cast<const float**>(misc + 128);
     float* d_mean = reinterpret_cast<float*>(misc + 136);
+    // pass-1 CTA ticket: zero in the module image, re-armed by every launch's last CTA
+    uint32_t* d_ticket = reinterpret_cast<uint32_t*>(misc + 144);
 
     if (d.table_n != p.n) {
         // New length: choose the kernels and refill the tables (the tables of
         // the previous length are overwritten; set-up calls are not capturable).
         LengthPlan lp;
-        std::string e = choose_length_plan(p.n, lp);
+        std::string e = choose_length_plan(p.n, lp, 0, 0, false);  // the built-in plan: no plan file read here
         if (!e.empty()) return static_fail(BRP_E_RUNTIME, e.c_str());
         if (!lp.fused) return static_fail(BRP_E_ARGUMENT, "no fused plan for this length");
         size_t off[12];
@@ -110,11 +140,8 @@ extern "C" int brp_cuda_search_static(const brp_params* params, const float* inp
         d.table_n = p.n;
     }
     const LengthPlan& lp = d.lp;
-    if (cudaMemcpyAsync(d_params, &p, sizeof(brp_params), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(d_input, &input, sizeof(input), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemsetAsync(count, 0, sizeof(uint32_t), s) != cudaSuccess ||
-        cudaMemsetAsync(status, 0, sizeof(uint32_t), s) != cudaSuccess)
-        return static_fail(BRP_E_RUNTIME, "argument upload failed");
+    static_args_kernel<<<1, 1, 0, s>>>(p, input, d_params, d_input, count, status);
+    if (cudaGetLastError() != cudaSuccess) return static_fail(BRP_E_RUNTIME, "argument kernel launch failed");
 
     FusedArgs a{};
     a.inputs = d_input;
@@ -123,7 +150,7 @@ extern "C" int brp_cuda_search_static(const brp_params* params, const float* inp
     a.work = work; a.work_stride = lp.M;
     a.power = power; a.power_stride = lp.M;
     a.partial = partial; a.partial_stride = lp.blocks1();
-    a.mean = d_mean; a.status = status; a.counts = count; a.cands = candidates;
+    a.mean = d_mean; a.tickets = d_ticket; a.status = status; a.counts = count; a.cands = candidates;
     a.capacity = capacity;
     a.snap = -1;
     const uint32_t span = p.fundamental > p.harmonic + 8 ? p.fundamental : p.harmonic + 8;

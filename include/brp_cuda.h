@@ -116,6 +116,18 @@ int brp_cuda_device_info(brp_ctx* ctx, char* buffer, size_t length);
 uint64_t brp_cuda_allocated_bytes(const brp_ctx* ctx);
 int brp_cuda_profile_counters(brp_ctx* ctx, char* buffer, size_t length);
 const char* brp_cuda_last_error(const brp_ctx* ctx);
+/* Replaces the unbounded fence wait of GPU::run (src/vulkan.cpp:306,
+ * vkWaitForFences with UINT64_MAX).  host_seconds (0..86400, default 300) is
+ * the deadline of brp_cuda_run's wait: past it the run returns BRP_E_TIMEOUT
+ * while the GPU finishes the work, and the next call on the context first
+ * waits (again bounded) for that work before it reuses the buffers.
+ * device_polls (default 4194304) bounds a kernel's first wait for its own
+ * asynchronous work (the harmonic kernel's staging copies, the tensor-core
+ * pass-1 MMAs); on expiry the template's status gets BRP_STATUS_WAIT_TIMEOUT,
+ * the kernel drains that work with the full bound and the run reports
+ * BRP_E_RESULT.  device_polls = 0 gives up at once (tests use it to exercise
+ * that path). */
+int brp_cuda_set_wait_limits(brp_ctx* ctx, uint32_t device_polls, double host_seconds);
 
 /* ---- Bank extension: a whole orbital bank over series of different lengths,
  * run as one captured CUDA graph (the batched form of src/workunit_main.cpp:77-93).
@@ -160,6 +172,40 @@ int brp_cuda_bank_set_toplist_filter(brp_bank* bank, uint32_t rows);
  * BF16 DFT products; kind 3 is never a default and is selected by id).
  * Returns the total count; writes at most cap entries. */
 int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* kinds, uint32_t cap);
+/* Autotuner for C callers.  The reference fixes its kernel variant by
+ * command-line options (workgroup, tile, radix and store variants of
+ * src/main.cpp and src/workunit_main.cpp:70); here, for every length class of
+ * the templates, each compiled pass-1 / pass-2 pair covering n (CUDA-core
+ * forms), each group size (groups[group_count], NULL: 16, 32, 64, 128) and 1 or
+ * 2 launch chains is timed over `reps` replays of the bank's captured graph of
+ * these templates with L2 flushed before each (CUDA events on the bank's
+ * stream); the bank is left configured with the fastest.  cache_path (NULL:
+ * none) is a JSON plan file shared with the Python tuner, keyed by device,
+ * n and template count: with BRP_TUNE_USE_CACHE an entry there is used without
+ * timing; new results are merged into it.  Every result also becomes the
+ * default plan of that length for brp::GPU contexts and banks created later in
+ * the process.  results[cap] receives one entry per length, *found their
+ * number.  Allocates an L2 flush buffer (512 MiB) while it runs. */
+typedef struct brp_tune_result {
+    double ms;  /* device time of one replay of the bank with this plan */
+    uint32_t n;
+    int32_t pass1, pass2;
+    uint32_t group, chains, tried, cached, reserved;
+} brp_tune_result;
+enum { BRP_TUNE_USE_CACHE = 1u };
+int brp_cuda_bank_autotune(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count,
+                           uint32_t reps, const uint32_t* groups, uint32_t group_count, const char* cache_path,
+                           uint32_t flags, brp_tune_result* results, uint32_t cap, uint32_t* found);
+/* Merges a plan file (written by brp_cuda_bank_autotune or the Python tuner)
+ * into the plans that default choices consult: for a length with a plan for
+ * the current device, brp_cuda_create, brp_cuda_bank_create and the static
+ * search take its pass pair (banks also its group and chains) instead of the
+ * built-in pairs.  NULL: $BRP_PLAN_CACHE, else ~/.cache/brp_b200/plans.json
+ * (which the library also reads by itself before its first default choice);
+ * "" forgets every plan (the built-in pairs again) and reads no file later. */
+int brp_cuda_load_plan_cache(const char* path);
+/* Message of the calling thread's last failed autotune / plan-cache call. */
+const char* brp_cuda_autotune_error(void);
 /* Device-only replay of the last brp_cuda_bank_run's graph (no host copies,
  * no wait): the throughput kernel time is measured around this by the caller
  * with events on brp_cuda_bank_stream().  brp_cuda_bank_configure and
@@ -176,6 +222,16 @@ int brp_cuda_bank_profile(brp_bank* bank, double* kernel_ms, uint32_t* launches)
 /* Kernels launched by one replay (for launch accounting). */
 uint32_t brp_cuda_bank_kernels_per_run(const brp_bank* bank);
 const char* brp_cuda_bank_last_error(const brp_bank* bank);
+/* brp_cuda_set_wait_limits for a bank (the same replacement of
+ * src/vulkan.cpp:306): host_seconds bounds brp_cuda_bank_run's and
+ * brp_cuda_bank_profile's waits, device_polls is a launch argument of the
+ * captured kernels (a change re-captures at the next run). */
+int brp_cuda_bank_set_wait_limits(brp_bank* bank, uint32_t device_polls, double host_seconds);
+/* No counterpart in the reference; a test aid for the error paths.  The
+ * `after`-th device allocation from now on (1 = the next one) made by a context
+ * or a bank reports failure without calling cudaMalloc; 0 turns it off.
+ * Process-wide. */
+void brp_cuda_debug_fail_allocation(uint32_t after);
 
 /* ---- Search without device allocation ----
  * No counterpart in the reference.  For callers that may not allocate device
@@ -186,19 +242,23 @@ const char* brp_cuda_bank_last_error(const brp_bank* bank);
  * summing, candidate compaction) with all working memory in a static device
  * array inside this library (about 4.2 MiB, held by every GPU that loads the
  * library until the process exits).  It calls no cudaMalloc or cudaFree.
- *   input      device, params->unpadded floats (the series)
- *   power      device, n/2 floats (P[k] = |X_k|^2 / n, P[0] = 0)
- *   candidates device, capacity entries; *count (device) the number found,
- *              which may exceed capacity; *status (device) BRP_STATUS_* bits
+ *   input      device, params->unpadded floats (the series), 4-byte aligned
+ *   power      device, n/2 floats (P[k] = |X_k|^2 / n, P[0] = 0), 16-byte aligned
+ *   candidates device, capacity entries, 16-byte aligned; *count (device,
+ *              4-byte aligned) the number found, which may exceed capacity;
+ *              *status (device, 4-byte aligned) BRP_STATUS_* bits
  *   stream     cudaStream_t (NULL: legacy default stream)
- * Series lengths 8192..1048576 (2^k or 3*2^k); longer ones are rejected with
- * BRP_E_ARGUMENT.  The call is asynchronous on `stream`; results are valid
- * once the stream has completed.  The first call on a device (and the first
- * call with a new series length) does set-up -- the scratch array's device
- * address, kernel attributes, the twiddle tables copied into the array --
- * so it must come before any stream capture.  Every call shares the one
- * array, which keeps the last call's contents: calls that overlap on the GPU
- * (other streams, other threads) race and must be serialised by the caller.
+ * Series lengths 8192..1048576 (2^k or 3*2^k); longer ones, and misaligned
+ * buffers, are rejected with BRP_E_ARGUMENT before any device work.  The call
+ * is asynchronous on `stream`; results are valid once the stream has
+ * completed.  The first call on a device (and the first call with a new series
+ * length) does set-up -- the scratch array's device address, kernel
+ * attributes, the twiddle tables copied into the array -- so that first call
+ * should come before any stream capture.  Every call shares the one array,
+ * which keeps the last call's contents: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  The
+ * set-up belongs to the device's context: do not call this again on a device
+ * after cudaDeviceReset in the same process.
  * brp_cuda_search_static_error() gives the calling thread's last message. */
 int brp_cuda_search_static(const brp_params* params, const float* input, float* power, brp_candidate* candidates,
                            uint32_t capacity, uint32_t* count, uint32_t* status, void* stream);

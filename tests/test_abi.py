@@ -100,3 +100,53 @@ def test_argument_errors_of_the_whitening_and_filter_entry_points():
         whiten.preprocess_dd(np.zeros(5000, np.uint8), 9999, True, 2.0, 16384, 128.0, 1.0, 1000)
     L = lib()
     assert L.brp_cuda_bank_set_toplist_filter(ctypes.c_void_p(0), 100) == 4
+
+
+def test_static_search_rejects_misaligned_buffers():
+    """brp_cuda_search_static checks the alignment its kernels need (16 bytes
+    for the power spectrum and the candidates, 4 for the rest) before any
+    device work, so a misaligned view is an argument error, not a fault."""
+    import ctypes
+    from brp_b200._lib import as_params, lib
+    p = as_params(B.parameters(1 << 16, (1 << 16) - 17, 0.3, 3600.0, 1.1, 128e-6))
+    L = lib()
+    ok, word = 1 << 12, 1 << 12  # aligned stand-in addresses (never dereferenced)
+    cases = [(ok, ok + 4, ok, word, word), (ok, ok, ok + 8, word, word), (ok + 2, ok, ok, word, word),
+             (ok, ok, ok, word + 1, word), (ok, ok, ok, word, word + 2)]
+    for inp, power, cands, count, status in cases:
+        st = L.brp_cuda_search_static(ctypes.byref(p), ctypes.c_void_p(inp), ctypes.c_void_p(power),
+                                      ctypes.c_void_p(cands), 16, ctypes.c_void_p(count), ctypes.c_void_p(status),
+                                      None)
+        assert st == 4
+        assert b"aligned" in L.brp_cuda_search_static_error()
+
+
+def test_wait_limit_entry_points_check_their_arguments():
+    import ctypes
+    from brp_b200._lib import lib
+    L = lib()
+    assert L.brp_cuda_set_wait_limits(ctypes.c_void_p(0), 10, 1.0) == 4
+    assert L.brp_cuda_bank_set_wait_limits(ctypes.c_void_p(0), 10, 1.0) == 4
+    L.brp_cuda_debug_fail_allocation(0)  # off: a no-op without a device
+
+
+def test_plan_file_is_read_without_a_device(tmp_path):
+    """The plan file shared with the Python tuner (json.dump of
+    {key: {pass1, pass2, group, chains, ms}}) is accepted; a malformed one or a
+    missing one is an argument error; "" resets to the built-in plans."""
+    import json
+    from brp_b200._lib import lib
+    L = lib()
+    good = tmp_path / "plans.json"
+    json.dump({"B200/sm100/148|n=4194304|templates=512": {"chains": 1, "group": 128, "ms": 15.4, "pass1": 110,
+                                                          "pass2": 202},
+               "B200/sm100/148|n=6291456|templates=128": {"pass1": 119, "pass2": 204, "group": 128, "chains": 2,
+                                                          "ms": 7.5, "tried": [1, 2, {"x": None}]}},
+              open(good, "w"), indent=1, sort_keys=True)
+    assert L.brp_cuda_load_plan_cache(str(good).encode()) == 0
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"k": {"pass1": 1, "pass2": }')
+    assert L.brp_cuda_load_plan_cache(str(bad).encode()) == 4
+    assert b"invalid plan cache" in L.brp_cuda_autotune_error()
+    assert L.brp_cuda_load_plan_cache(str(tmp_path / "missing.json").encode()) == 4
+    assert L.brp_cuda_load_plan_cache(b"") == 0

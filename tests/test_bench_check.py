@@ -66,3 +66,34 @@ def test_check_reports_differences(setup):
     assert not out["resampled_template0_bit_exact"]
     assert out["candidates_differ"] == 1 and out["candidates_differ_away_from_threshold"] == 1
     assert out["max_power_rel_diff_shared"] > 9e-4
+
+
+def test_reference_arm_templates_equal_the_cuda_arms(oracle):
+    """The reference arm builds its bank with the reference's own
+    search_parameters; the templates are byte-identical to the CUDA arm's
+    (this package's host code), so both arms search the same bank."""
+    from brp_b200 import synth
+    mine = synth.bank_workload("t", [1 << 16], [24], [1], seed=3)
+    ref = synth.bank_workload("t", [1 << 16], [24], [1], seed=3, search=bench.reference_search())
+    assert [bytes(p) for p in mine.templates] == [bytes(p) for p in ref.templates]
+    assert np.array_equal(mine.series[0], ref.series[0])
+
+
+def test_reference_arm_runs_without_the_cuda_library(tmp_path):
+    """`bench.py --impl reference` (a small bank) prints its line and never maps
+    this repository's CUDA library into the process."""
+    import json
+    import subprocess
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--templates', '8', '--steps', '1', "
+            "'--warmup', '1']; runpy.run_path(%r, run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); print('MAPPED' if 'libbrp_cuda' in maps else 'CLEAN')"
+            % os.path.join(ROOT, "bench.py"))
+    out = subprocess.run([sys.executable, "-c", code], cwd=str(tmp_path), capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.strip().splitlines()
+    assert lines[-1] == "CLEAN"
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["config"]["templates_per_step"] == 8
+    assert line["config"]["workload"] == bench.workload_name(8)
+    assert line["value"] > 0 and line["e2e"]["h2d_bytes_per_step"] == 0

@@ -159,7 +159,9 @@ def _config_pairs():
     for i1, L1 in p1:
         for i2, L2 in p2:
             n = 2 * L1 * L2
-            if n <= (3 << 22) and (n <= (1 << 22) or (i1, i2) == (106, 204)):
+            # every pair up to the mixed-radix bench length 3*2^21 (1536 x 2048 and
+            # 3072 x 1024), and one pair at the longest supported length 3*2^22
+            if n <= (3 << 21) or (i1, i2) == (106, 204):
                 out.append((i1, i2, n))
     return out
 

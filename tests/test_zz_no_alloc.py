@@ -70,7 +70,7 @@ def assert_same(got, ref, p):
             assert abs(v - thr) <= THRESH_RTOL * thr, (k, v, thr)
 
 
-def test_static_search_matches_regular_entry_point():
+def test_static_search_matches_regular_entry_point(oracle):
     cases = [
         (1 << 20, synth.Pulsar(311.0, 9000.0, 1.3, 0.7, 0.02, 8, 0.1), 5, True),
         (1 << 20, synth.Pulsar(97.0, 5000.0, 0.4, 2.9, 0.03, 5, 0.1), 6, False),  # second call, same array
@@ -85,6 +85,9 @@ def test_static_search_matches_regular_entry_point():
         got = static_search(p, x)
         ref = regular_search(p, x)
         assert_same(got, ref, p)
+        # harmonic sums and candidate selection of its own power spectrum are
+        # exactly the restated reference's (shaders/harmonic.comp, select)
+        assert np.array_equal(got[1], oracle.select(oracle.harmonic(got[0], p), p))
         found += len(ref[1])
     assert found > 0
 
