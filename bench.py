@@ -71,6 +71,8 @@ def parse():
                    help="pass1,pass2,group,chains: use this configuration instead of the autotuner")
     a.add_argument("--toplist-rows", type=int, default=100,
                    help="device toplist pre-filter rows per level (0: return every candidate)")
+    a.add_argument("--same-device", action="store_true",
+                   help="every rank on device 0 (the multi-rank flow on one GPU; needs --dist-backend gloo)")
     a.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
                    help="process-group backend of the multi-rank run (the search has no data-path collective)")
     a.add_argument("--workload", default="bank", choices=["bank", "mixed-radix", "uneven"],
@@ -346,6 +348,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.same_device:
+        local = 0  # the ranks share one GPU; their kernels never wait on one another
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload != "bank":

@@ -87,13 +87,20 @@ __device__ __forceinline__ void post_pair(const PostArgs& c, uint32_t k, uint32_
     const float2 hf = twiddle2(c.hf_hi, c.hf_lo, kSplitLog2, k);
     const float cv = hf.x, sv = -hf.y;
     const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
-    const float2 wm = make_float2(-w.x, w.y);
-    const float2 wam = c.a_odd ? make_float2(-wa.x, wa.y) : make_float2(wa.x, -wa.y);
-    const float2 G1 = cmul(make_float2(1.f - wa.x, -wa.y), make_float2(sv, -cv));
-    const float2 G2 = cmul(make_float2(1.f - wam.x, -wam.y), make_float2(cv, -sv));
-    const float f1 = __fdividef(c.hm, sv), f2 = __fdividef(c.hm, cv);
-    const float2 X1 = real_bin(zk, zm, w, make_float2(G1.x * f1, G1.y * f1));
-    const float2 X2 = real_bin(zm, zk, wm, make_float2(G2.x * f2, G2.y * f2));
+    // X_k and X_{M-k} share s = Z_k + Z*_{M-k}, d = Z_k - Z*_{M-k} and t = W d
+    // (for the mirror bin: s' = s*, d' = -d*, W' = -W*, so W' d' = t*)
+    const float2 s = make_float2(zk.x + zm.x, zk.y - zm.y);
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+    const float2 t = cmul(w, d);
+    // padding terms mean G_k = hm (1 - W_n^{k steps}) (1 - i cot(pi k / n)) and
+    // mean G_{M-k} = hm (1 - W_n^{(M-k) steps}) (1 - i tan(pi k / n))
+    const float a1 = 1.f - wa.x, b1 = -wa.y;
+    const float a2 = c.a_odd ? 1.f + wa.x : 1.f - wa.x, b2 = c.a_odd ? -wa.y : wa.y;
+    const float cot = __fdividef(cv, sv), tan = __fdividef(sv, cv);
+    const float2 X1 = make_float2(__fmaf_rn(0.5f, s.x + t.y, c.hm * __fmaf_rn(b1, cot, a1)),
+                                  __fmaf_rn(0.5f, s.y - t.x, c.hm * __fmaf_rn(-a1, cot, b1)));
+    const float2 X2 = make_float2(__fmaf_rn(0.5f, s.x - t.y, c.hm * __fmaf_rn(b2, tan, a2)),
+                                  __fmaf_rn(0.5f, -s.y - t.x, c.hm * __fmaf_rn(-a2, tan, b2)));
     const float p1 = X1.x * X1.x + X1.y * X1.y, p2 = X2.x * X2.x + X2.y * X2.y;
     c.Pw[k] = c.pow2 ? p1 * c.inv_n : p1 / c.fn;
     c.Pw[km] = c.pow2 ? p2 * c.inv_n : p2 / c.fn;

@@ -23,6 +23,7 @@
 // previous thread's last bins, whose maximum and first value arrive by warp
 // shuffle (and through shared memory across warps).  Thread 0 of each CTA only
 // computes that halo for thread 1.
+#include <cooperative_groups.h>
 #include "async_device.cuh"
 #include "brp_internal.h"
 
@@ -105,9 +106,16 @@ __device__ __forceinline__ void add_factor(float (&t)[16], const float* stage, c
 
 struct LevelTail { float best, first; };
 
+// Appends one candidate to the template's list.  The lanes of a warp that emit
+// together take their slots with one atomic add of the leader (warp-aggregated
+// compaction); the list order is arbitrary and sorted by (level, bin) later.
 __device__ __forceinline__ void emit(uint32_t j, uint32_t h, float v, uint32_t* count, brp_candidate* out,
                                      uint32_t capacity, uint32_t* status) {
-    uint32_t slot = atomicAdd(count, 1u);
+    namespace cg = cooperative_groups;
+    const cg::coalesced_group active = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (active.thread_rank() == 0) base = atomicAdd(count, active.size());
+    const uint32_t slot = active.shfl(base, 0) + active.thread_rank();
     if (slot < capacity) {
         brp_candidate c;
         c.bin = j; c.level = h; c.power = v; c.reserved = 0;

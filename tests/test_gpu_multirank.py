@@ -74,3 +74,22 @@ def test_two_ranks_on_one_gpu_equal_one_rank(bank_filter):
     one = search(bank_filter, 0, 1)
     assert len(one) > 0
     assert two.tobytes() == one.tobytes()
+
+
+def test_bench_multirank_path_on_one_gpu():
+    """bench.py's own multi-rank path under torchrun (two gloo ranks sharing
+    the GPU): template shards, barriers, max-over-ranks timing and the
+    end-to-end step with the gather to rank 0 and the bank-wide fold."""
+    import json
+    import subprocess
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.join(ROOT, "bench.py"),
+           "--gpus", "2", "--dist-backend", "gloo", "--same-device", "--templates", "16", "--steps", "2",
+           "--warmup", "3", "--no-cpu-baseline", "--no-plain", "--no-tune"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-3000:]
+    lines = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1  # rank 0 alone prints
+    line = lines[0]
+    assert line["n_gpus"] == 2 and line["config"]["parallelism"] == "template shards, 2 rank(s)"
+    assert line["config"]["templates_per_gpu"] == 16 and line["value"] > 0 and line["e2e"]["value"] > 0
