@@ -595,11 +595,11 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
             cb.group = std::min(cp.group, max_templates);
             cb.chains = std::min<uint32_t>(std::max<uint32_t>(cp.chains, 1), 2);
         }
-        cb.capacity = cb.group * cb.chains;
+        cb.capacity = cb.group * cb.chains;  // every chain has its own intermediates
         cb.partial_per_template = std::max<uint32_t>(lp.blocks1(), lp.M / 64);
-        if ((st = b->alloc(&cb.work, size_t(cb.group) * lp.M, "work")) ||
-            (st = b->alloc(&cb.power, size_t(cb.group) * lp.M, "power")) ||
-            (st = b->alloc(&cb.partial, size_t(cb.group) * cb.partial_per_template, "partial")))
+        if ((st = b->alloc(&cb.work, size_t(cb.capacity) * lp.M, "work")) ||
+            (st = b->alloc(&cb.power, size_t(cb.capacity) * lp.M, "power")) ||
+            (st = b->alloc(&cb.partial, size_t(cb.capacity) * cb.partial_per_template, "partial")))
             return cleanup(st);
         b->classes[kv.first] = cb;
     }
@@ -745,6 +745,10 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     }
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t x, uint32_t y) { return b->n[series_of[x]] > b->n[series_of[y]]; });
+    // every chain of a class writes its own group of intermediates
+    for (const auto& kv : b->classes)
+        if (uint64_t(kv.second.group) * kv.second.chains > kv.second.capacity)
+            return b->fail(BRP_E_RUNTIME, "bank class buffers smaller than its groups and chains");
     std::vector<uint32_t> sorted_n(count), spans(count);
     std::vector<uint64_t> key;
     key.push_back(count);

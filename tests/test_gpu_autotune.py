@@ -94,3 +94,30 @@ def test_python_written_plan_file_steers_the_default_choice(tmp_path, workload):
             assert len(cands) > 0 and near_threshold_only(cands, ref, p)
     finally:
         tune.load_plans("")  # later tests get the built-in pairs
+
+
+def test_bank_created_under_a_two_chain_plan(tmp_path, workload):
+    """A new bank takes the cached plan's templates per launch and chains
+    (each chain with its own intermediate buffers) and finds exactly what a
+    bank configured with the same plan by hand finds."""
+    wl = workload
+    key = "%s|n=%d|templates=%d" % (tune._device_key(), N, 100000)
+    path = str(tmp_path / "plans-chains.json")
+    with open(path, "w") as f:
+        json.dump({key: {"pass1": 117, "pass2": 201, "group": 8, "chains": 2, "ms": 1.0}}, f)
+    try:
+        tune.load_plans(path)
+        bank = B.Bank(wl.n, [len(x) for x in wl.series], len(wl.templates), 8192)
+        bank.set_series(0, wl.series[0])
+        got, _, status = bank.run(wl.templates)
+        assert not status.any() and bank.kernels_per_run == 3 * 4 + 1  # 32 templates in 4 groups of 8
+        bank.close()
+    finally:
+        tune.load_plans("")
+    ref_bank = B.Bank(wl.n, [len(x) for x in wl.series], len(wl.templates), 8192)
+    ref_bank.set_series(0, wl.series[0])
+    ref_bank.configure(N, pass1=117, pass2=201, group=8, chains=2)
+    ref, _, _ = ref_bank.run(wl.templates)
+    ref_bank.close()
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
