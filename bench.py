@@ -9,9 +9,11 @@ Reported (one JSON line, rank 0):
   value      templates/s over all ranks, device-resident inputs, one captured
              CUDA graph per step, L2 flushed between steps (CUDA events on the
              bank's stream, max over ranks)
-  e2e        the same metric through the public API (Bank.run) with the
-             series copied from pinned host memory every step, candidates copied
-             back and folded into the bank-wide toplist on the host
+  e2e        the same metric through the public API (Bank.submit / Bank.wait)
+             with the series copied from pinned host memory every step,
+             candidates copied back and folded into the bank-wide toplist on
+             the host; one step's upload and fold overlap its neighbours'
+             kernels
   roofline   the dominant kernel's algorithmic bytes / its device time, and
              its ncu DRAM bytes / its device time
   plain      templates/s of the step-by-step per-template pipeline, same GPU
@@ -402,6 +404,22 @@ def main():
         bank.set_series(0, x_host)
         return shard.search_and_fold(bank, tarr, begin, all_tarr, all_orbits, out=outbuf)
 
+    def e2e_pipelined(steps):
+        # The same work per step through the asynchronous half of the API: step
+        # k + 1's series upload (pinned memory, the copy stream, into the buffer
+        # step k does not read) crosses PCIe while step k's kernels run, and
+        # step k's candidate download is followed by step k + 1's submit before
+        # step k's toplist fold on the host.
+        bank.set_series(0, x_host)
+        bank.submit(tarr)
+        for k in range(steps):
+            if k + 1 < steps:
+                bank.set_series(0, x_host)
+            flat, offs, counts, status = bank.wait(out=outbuf)
+            if k + 1 < steps:
+                bank.submit(tarr)
+            B.Toplist().fold(tarr, orbits, flat, counts)
+
     # autotune the kernel configuration and templates per launch on this bank
     # (untimed), then warm up through the public API (captures the graph)
     plan = None
@@ -451,8 +469,11 @@ def main():
     # --- end to end through the public API (series H2D + candidates D2H + toplist)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_fold_step()
+    if world == 1:
+        e2e_pipelined(args.steps)
+    else:
+        for _ in range(args.steps):
+            e2e_fold_step()
     torch.cuda.synchronize()
     e2e_ms = 1000 * (time.perf_counter() - t0)
     barrier()

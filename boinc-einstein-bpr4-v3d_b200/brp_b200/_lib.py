@@ -86,7 +86,7 @@ EXPORTS = (
     "brp_cuda_preprocess", "brp_cuda_preprocess_dd", "brp_cuda_preprocess_error", "brp_host_read_zap",
     "brp_host_zap_noise", "brp_host_error", "brp_cuda_set_wait_limits", "brp_cuda_bank_set_wait_limits",
     "brp_cuda_debug_fail_allocation", "brp_cuda_bank_autotune", "brp_cuda_load_plan_cache",
-    "brp_cuda_autotune_error",
+    "brp_cuda_autotune_error", "brp_cuda_bank_submit", "brp_cuda_bank_wait",
 )
 
 
@@ -122,6 +122,8 @@ def lib():
             L.brp_cuda_bank_destroy.restype = None
             L.brp_cuda_bank_set_series.argtypes = [vp, u32, vp]
             L.brp_cuda_bank_run.argtypes = [vp, vp, vp, u32, vp, u64, vp, vp]
+            L.brp_cuda_bank_submit.argtypes = [vp, vp, vp, u32]
+            L.brp_cuda_bank_wait.argtypes = [vp, vp, u64, vp, vp]
             L.brp_cuda_search_static.argtypes = [P, vp, vp, vp, u32, vp, vp, vp]
             L.brp_cuda_search_static_error.restype = ctypes.c_char_p
             L.brp_cuda_bank_launch.argtypes = [vp]

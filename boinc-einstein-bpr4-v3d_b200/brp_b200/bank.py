@@ -55,15 +55,32 @@ class Bank:
         """As run(), returning the candidates back to back: (candidates,
         offsets[count + 1], counts, status).  `templates` may be a list of
         Params or an array from params_array()."""
+        self.submit(templates, series_of)
+        return self.wait(out)
+
+    def submit(self, templates, series_of=None):
+        """Enqueues a run of the bank and returns at once (brp_cuda_bank_submit);
+        wait() collects it.  set_series() meanwhile uploads into the buffer the
+        run does not read, for the next submit."""
         arr = templates if isinstance(templates, ctypes.Array) else self.params_array(templates)
         count = len(arr)
         so = np.zeros(count, np.uint32) if series_of is None else np.ascontiguousarray(series_of, dtype=np.uint32)
+        check(lib().brp_cuda_bank_submit(self._b, arr, ptr(so), count), self._err)
+        self._submitted = count
+
+    def wait(self, out=None):
+        """Blocks until the submitted run is done: (candidates, offsets[count + 1],
+        counts, status) as run_flat()."""
+        count = getattr(self, "_submitted", 0)
+        if not count:
+            raise BrpError(4, "no submitted run to wait for")
+        self._submitted = 0
         counts = np.zeros(count, np.uint32)
         status = np.zeros(count, np.uint32)
         cap = count * self.capacity
         if out is None:
             out = np.empty(cap, CANDIDATE)
-        st = lib().brp_cuda_bank_run(self._b, arr, ptr(so), count, ptr(out), out.size, ptr(counts), ptr(status))
+        st = lib().brp_cuda_bank_wait(self._b, ptr(out), out.size, ptr(counts), ptr(status))
         if st and st != 2:
             check(st, self._err)
         offs = np.zeros(count + 1, np.int64)

@@ -440,7 +440,16 @@ struct brp_bank {
     cudaStream_t side = nullptr;  // second chain of the graph
     cudaEvent_t fork = nullptr, join = nullptr;
     std::vector<uint32_t> n, unpadded;
-    std::vector<float*> d_series;
+    // Two device buffers per series: an upload while a submitted run is in
+    // flight goes to the buffer that run does not read (on the copy stream,
+    // ordered before the next run by an event).
+    std::vector<float*> d_series[2];
+    std::vector<int> latest;              // per series: buffer holding the latest upload
+    std::vector<int> in_use;              // per series: buffer the in-flight run reads (-1: none)
+    std::vector<cudaEvent_t> series_ready;
+    cudaStream_t copy = nullptr;
+    bool inflight = false;                // a submitted run awaits brp_cuda_bank_wait
+    std::vector<uint32_t> run_order;      // the in-flight run's slot -> caller index
     std::map<uint32_t, LengthPlan> plans;  // by n
     struct ClassBuffers {
         float2* work = nullptr;
@@ -520,7 +529,10 @@ struct brp_bank {
     }
     ~brp_bank() {
         cudaSetDevice(device);
+        if (copy) cudaStreamSynchronize(copy);
         if (stream) cudaStreamSynchronize(stream);
+        for (auto e : series_ready) cudaEventDestroy(e);
+        if (copy) cudaStreamDestroy(copy);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (done) cudaEventDestroy(done);
@@ -566,7 +578,8 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return cleanup(st);
     if ((st = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) return cleanup(st);
     if ((st = b->cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "cudaEventCreate"))) return cleanup(st);
-    if ((st = b->cuda(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+    if ((st = b->cuda(cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (st = b->cuda(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
         (st = b->cuda(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate")) ||
         (st = b->cuda(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming), "cudaEventCreate")))
         return cleanup(st);
@@ -576,9 +589,16 @@ extern "C" int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, co
     b->capacity = capacity;
     for (uint32_t s = 0; s < series_count; ++s) {
         if (unpadded[s] < 2 || unpadded[s] > n[s]) return b->fail(BRP_E_ARGUMENT, "invalid series length"), cleanup(BRP_E_ARGUMENT);
-        float* d = nullptr;
-        if ((st = b->alloc(&d, unpadded[s], "series"))) return cleanup(st);
-        b->d_series.push_back(d);
+        float *d0 = nullptr, *d1 = nullptr;
+        cudaEvent_t ev = nullptr;
+        if ((st = b->alloc(&d0, unpadded[s], "series")) || (st = b->alloc(&d1, unpadded[s], "series")) ||
+            (st = b->cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate")))
+            return cleanup(st);
+        b->d_series[0].push_back(d0);
+        b->d_series[1].push_back(d1);
+        b->series_ready.push_back(ev);
+        b->latest.push_back(0);
+        b->in_use.push_back(-1);
         if (!b->plans.count(n[s])) {
             std::string e = make_length_plan(n[s], b->plans[n[s]], b->stream);
             if (!e.empty()) { b->fail(BRP_E_ARGUMENT, e); return cleanup(BRP_E_ARGUMENT); }
@@ -628,11 +648,18 @@ extern "C" void brp_cuda_bank_destroy(brp_bank* b) { delete b; }
 
 extern "C" int brp_cuda_bank_set_series(brp_bank* b, uint32_t s, const float* input) {
     if (!b || !input) return set_thread_error(BRP_E_ARGUMENT, "null argument");
-    if (s >= b->d_series.size()) return b->fail(BRP_E_ARGUMENT, "series index out of range");
+    if (s >= b->latest.size()) return b->fail(BRP_E_ARGUMENT, "series index out of range");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
-    return b->cuda(cudaMemcpyAsync(b->d_series[s], input, size_t(b->unpadded[s]) * 4, cudaMemcpyHostToDevice, b->stream),
-                   "series upload");
+    // Into the buffer no in-flight run reads; runs submitted later read it.
+    const int target = b->in_use[s] >= 0 ? 1 - b->in_use[s] : b->latest[s];
+    if ((st = b->cuda(cudaMemcpyAsync(b->d_series[target][s], input, size_t(b->unpadded[s]) * 4,
+                                      cudaMemcpyHostToDevice, b->copy),
+                      "series upload")) ||
+        (st = b->cuda(cudaEventRecord(b->series_ready[s], b->copy), "series upload")))
+        return st;
+    b->latest[s] = target;
+    return BRP_OK;
 }
 
 // Records the whole bank search on b->stream (captured into the graph).  With
@@ -723,10 +750,11 @@ static void record_bank(brp_bank* b, const std::vector<uint32_t>& sorted_n, cons
     b->kernels_per_run = kernels + 1;
 }
 
-extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const uint32_t* series_of, uint32_t count,
-                                 brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status) {
-    if (!b || !templates || !series_of || !counts || !status) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+extern "C" int brp_cuda_bank_submit(brp_bank* b, const brp_params* templates, const uint32_t* series_of,
+                                    uint32_t count) {
+    if (!b || !templates || !series_of) return set_thread_error(BRP_E_ARGUMENT, "null argument");
     if (!count || count > b->max_templates) return b->fail(BRP_E_ARGUMENT, "template count outside 1..max_templates");
+    if (b->inflight) return b->fail(BRP_E_ARGUMENT, "a submitted run awaits brp_cuda_bank_wait");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
     // The pinned staging buffers below are the sources and targets of the
@@ -759,12 +787,18 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
         if (b->h_slot_series) b->h_slot_series[k] = series_of[t];
         b->h_params[k] = templates[t];
         b->h_params[k].capacity = b->capacity;
-        b->h_inputs[k] = b->d_series[series_of[t]];
+        b->h_inputs[k] = b->d_series[b->latest[series_of[t]]][series_of[t]];
         sorted_n[k] = b->n[series_of[t]];
         spans[k] = std::max(templates[t].fundamental, templates[t].harmonic + 8);
         key.push_back((uint64_t(sorted_n[k]) << 32) | spans[k]);
     }
     cudaStream_t s = b->stream;
+    // the series uploads (copy stream) before the run
+    std::vector<char> used(b->latest.size(), 0);
+    for (uint32_t t = 0; t < count; ++t) used[series_of[t]] = 1;
+    for (size_t q = 0; q < used.size(); ++q)
+        if (used[q] && (st = b->cuda(cudaStreamWaitEvent(s, b->series_ready[q], 0), "series upload wait")))
+            return st;
     if ((st = b->cuda(cudaMemcpyAsync(b->d_params, b->h_params, count * sizeof(brp_params), cudaMemcpyHostToDevice, s),
                       "params upload")) ||
         (st = b->cuda(cudaMemcpyAsync(b->d_inputs, b->h_inputs, count * sizeof(void*), cudaMemcpyHostToDevice, s),
@@ -795,11 +829,29 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     cudaMemcpyAsync(h_status, b->d_status, count * 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(b->h_offsets, b->d_offsets, (count + 1) * 8, cudaMemcpyDeviceToHost, s);
     if (b->filter_rows) cudaMemcpyAsync(b->h_kept, b->filter.kept, count * 4, cudaMemcpyDeviceToHost, s);
-    cudaEventRecord(b->done, s);
+    if ((st = b->cuda(cudaEventRecord(b->done, s), "bank search"))) return st;
+    for (size_t q = 0; q < used.size(); ++q) b->in_use[q] = used[q] ? b->latest[q] : -1;
+    b->run_order = order;
+    b->inflight = true;
+    return BRP_OK;
+}
+
+extern "C" int brp_cuda_bank_wait(brp_bank* b, brp_candidate* out, uint64_t out_cap, uint32_t* counts,
+                                  uint32_t* status) {
+    if (!b || !counts || !status) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (!b->inflight) return b->fail(BRP_E_ARGUMENT, "no submitted run to wait for");
+    int st;
+    if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
+    // The run is over for the caller whatever the outcome: its series buffers are free again.
+    b->inflight = false;
+    std::fill(b->in_use.begin(), b->in_use.end(), -1);
+    const std::vector<uint32_t>& order = b->run_order;
+    const uint32_t count = uint32_t(order.size());
+    uint32_t* h_status = b->h_counts + b->max_templates;
     bool timed_out = false;
     cudaError_t e = wait_event(b->done, b->wait_seconds, &timed_out);
     if (timed_out) {
-        b->pending = b->done;
+        b->pending = b->done;  // the next submit waits for it before it reuses the staging buffers
         return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
     }
     if ((st = b->cuda(e, "bank search"))) return st;
@@ -825,9 +877,22 @@ extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const
     return BRP_OK;
 }
 
+extern "C" int brp_cuda_bank_run(brp_bank* b, const brp_params* templates, const uint32_t* series_of, uint32_t count,
+                                 brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status) {
+    if (!b || !templates || !series_of || !counts || !status) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    const int st = brp_cuda_bank_submit(b, templates, series_of, count);
+    return st ? st : brp_cuda_bank_wait(b, out, out_cap, counts, status);
+}
+
+// Calls that change or read the bank's buffers wait until a submitted run is collected.
+static int refuse_inflight(brp_bank* b) {
+    return b->inflight ? b->fail(BRP_E_ARGUMENT, "a submitted run awaits brp_cuda_bank_wait") : BRP_OK;
+}
+
 extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, int32_t pass2, uint32_t group,
                                        uint32_t chains) {
     if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    if (refuse_inflight(b)) return BRP_E_ARGUMENT;
     auto it = b->plans.find(n);
     if (it == b->plans.end()) return b->fail(BRP_E_ARGUMENT, "no series of that length");
     int st;
@@ -866,6 +931,7 @@ extern "C" int brp_cuda_bank_configure(brp_bank* b, uint32_t n, int32_t pass1, i
 
 extern "C" int brp_cuda_bank_set_toplist_filter(brp_bank* b, uint32_t rows) {
     if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    if (refuse_inflight(b)) return BRP_E_ARGUMENT;
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
     if ((st = b->cuda(cudaStreamSynchronize(b->stream), "toplist filter"))) return st;
@@ -935,12 +1001,14 @@ extern "C" int brp_cuda_fast_configs(int32_t* ids, uint32_t* lengths, uint32_t* 
 
 extern "C" int brp_cuda_bank_launch(brp_bank* b) {
     if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    if (refuse_inflight(b)) return BRP_E_ARGUMENT;
     if (!b->exec) return b->fail(BRP_E_ARGUMENT, "no captured bank graph (run the bank after configuring it)");
     return b->cuda(cudaGraphLaunch(b->exec, b->stream), "graph launch");
 }
 
 extern "C" int brp_cuda_bank_profile(brp_bank* b, double* kernel_ms, uint32_t* launches) {
     if (!b || !kernel_ms) return set_thread_error(BRP_E_ARGUMENT, "null argument");
+    if (refuse_inflight(b)) return BRP_E_ARGUMENT;
     if (!b->last_count) return b->fail(BRP_E_ARGUMENT, "no bank run to profile");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) || (st = settle_pending(b))) return st;
@@ -986,6 +1054,7 @@ extern "C" int brp_cuda_set_wait_limits(brp_ctx* c, uint32_t device_polls, doubl
 
 extern "C" int brp_cuda_bank_set_wait_limits(brp_bank* b, uint32_t device_polls, double host_seconds) {
     if (!b) return set_thread_error(BRP_E_ARGUMENT, "null bank");
+    if (refuse_inflight(b)) return BRP_E_ARGUMENT;
     const uint32_t before = b->wait_polls;
     int st = set_wait_limits(b, device_polls, host_seconds);
     if (!st && before != device_polls) {

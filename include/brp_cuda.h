@@ -140,7 +140,11 @@ typedef struct brp_bank brp_bank;
 int brp_cuda_bank_create(uint32_t series_count, const uint32_t* n, const uint32_t* unpadded, uint32_t max_templates,
                          uint32_t capacity, int32_t device, brp_bank** out);
 void brp_cuda_bank_destroy(brp_bank* bank);
-/* Copies one series (unpadded[s] floats, host memory) to the device. */
+/* Copies one series (unpadded[s] floats, host memory) to the device,
+ * asynchronously on the bank's copy stream; the next submitted run waits for
+ * it.  From page-locked memory the copy overlaps the device's work, and the
+ * host buffer must then stay unchanged until the next run has completed; from
+ * pageable memory the call returns once the data is staged. */
 int brp_cuda_bank_set_series(brp_bank* bank, uint32_t series, const float* input);
 /* Runs count templates; template t searches series series_of[t] with
  * templates[t] (whose n/unpadded must equal that series').  Writes the
@@ -150,6 +154,19 @@ int brp_cuda_bank_set_series(brp_bank* bank, uint32_t series, const float* input
  * out_cap is too small.  Blocks until done. */
 int brp_cuda_bank_run(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count,
                       brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status);
+/* brp_cuda_bank_run in two halves, so a caller can overlap its own work with
+ * the device's (the reference's bank loop, src/workunit_main.cpp:77-93, waits
+ * on every batch): brp_cuda_bank_submit enqueues the run (templates are copied
+ * at the call) and returns; brp_cuda_bank_wait blocks until it is done and
+ * returns its results as brp_cuda_bank_run does.  One run at a time: a second
+ * submit, configure, toplist filter, profile, launch or wait-limit change
+ * before the wait is refused (BRP_E_ARGUMENT).  brp_cuda_bank_set_series is
+ * allowed meanwhile: each series has two device buffers, and an upload while
+ * a run is in flight goes to the buffer that run does not read (the next
+ * submit reads it), so the next step's series can cross PCIe while this step
+ * runs. */
+int brp_cuda_bank_submit(brp_bank* bank, const brp_params* templates, const uint32_t* series_of, uint32_t count);
+int brp_cuda_bank_wait(brp_bank* bank, brp_candidate* out, uint64_t out_cap, uint32_t* counts, uint32_t* status);
 /* Selects the kernels of one length class: compiled pass-1 / pass-2
  * configuration ids (0 = default, -1 = generic kernels), templates per
  * launch and independent launch chains in the graph (1 or 2; 0 = keep).

@@ -148,3 +148,45 @@ def test_configure_drops_the_graph_and_frees_replaced_buffers():
     assert 300 <= grown <= 500  # 64 x 6 MiB = 384 MiB (not 768)
     for a, b in zip(first, again):
         assert np.array_equal(a, b)
+
+
+def test_submit_wait_with_an_upload_in_flight(small_bank):
+    """brp_cuda_bank_submit / brp_cuda_bank_wait: a series uploaded while a run
+    is in flight goes to the other buffer, so that run still searches the old
+    series and the next one the new; calls that touch the bank's buffers are
+    refused until the wait."""
+    wl = small_bank
+    other = [x[::-1].copy() for x in wl.series]  # a different series of the same lengths
+
+    def fresh(series):
+        bank = B.Bank(wl.n, [len(x) for x in wl.series], len(wl.templates), 8192)
+        for s, x in enumerate(series):
+            bank.set_series(s, x)
+        return bank
+
+    ref_bank = fresh(wl.series)
+    ref_old, _, _ = ref_bank.run(wl.templates, wl.series_of)
+    ref_bank.close()
+    ref_bank = fresh(other)
+    ref_new, _, _ = ref_bank.run(wl.templates, wl.series_of)
+    ref_bank.close()
+
+    bank = fresh(wl.series)
+    bank.submit(wl.templates, wl.series_of)
+    for s, x in enumerate(other):
+        bank.set_series(s, x)  # while the run is in flight
+    with pytest.raises(B.BrpError) as e:
+        bank.configure(wl.n[0], group=4)
+    assert e.value.status == 4
+    with pytest.raises(B.BrpError):
+        bank.submit(wl.templates, wl.series_of)
+    flat, offs, counts, status = bank.wait()
+    assert not status.any()
+    for t, r in enumerate(ref_old):
+        assert np.array_equal(flat[offs[t]:offs[t + 1]], r)
+    got, _, _ = bank.run(wl.templates, wl.series_of)
+    for a, b in zip(got, ref_new):
+        assert np.array_equal(a, b)
+    with pytest.raises(B.BrpError):
+        bank.wait()
+    bank.close()
