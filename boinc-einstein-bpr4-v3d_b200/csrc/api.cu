@@ -96,6 +96,7 @@ struct brp_ctx {
     cudaEvent_t pending = nullptr;             // completion of a run that passed its deadline
     std::string error;
 
+    void run_finished() {}
     int fail(int code, const std::string& msg) {
         error = msg;
         g_thread_error = msg;
@@ -275,6 +276,7 @@ static int settle_pending(Obj* o) {
     cudaError_t e = wait_event(o->pending, o->wait_seconds, &timed_out);
     if (timed_out) return o->fail(BRP_E_TIMEOUT, "the previous run is still executing after the deadline");
     o->pending = nullptr;
+    o->run_finished();
     return o->cuda(e, "previous run");
 }
 
@@ -494,6 +496,8 @@ struct brp_bank {
     cudaEvent_t pending = nullptr;             // completion of a run that passed its deadline
     std::string error;
 
+    // A run has finished on the device: its series buffers may be written again.
+    void run_finished() { std::fill(in_use.begin(), in_use.end(), -1); }
     int fail(int code, const std::string& msg) {
         error = msg;
         g_thread_error = msg;
@@ -842,9 +846,10 @@ extern "C" int brp_cuda_bank_wait(brp_bank* b, brp_candidate* out, uint64_t out_
     if (!b->inflight) return b->fail(BRP_E_ARGUMENT, "no submitted run to wait for");
     int st;
     if ((st = b->cuda(cudaSetDevice(b->device), "cudaSetDevice"))) return st;
-    // The run is over for the caller whatever the outcome: its series buffers are free again.
+    // The run is over for the caller whatever the outcome.  Its series buffers
+    // stay marked in use until it has finished on the device (below, or when
+    // the next call settles a run that passed its deadline).
     b->inflight = false;
-    std::fill(b->in_use.begin(), b->in_use.end(), -1);
     const std::vector<uint32_t>& order = b->run_order;
     const uint32_t count = uint32_t(order.size());
     uint32_t* h_status = b->h_counts + b->max_templates;
@@ -854,6 +859,7 @@ extern "C" int brp_cuda_bank_wait(brp_bank* b, brp_candidate* out, uint64_t out_
         b->pending = b->done;  // the next submit waits for it before it reuses the staging buffers
         return b->fail(BRP_E_TIMEOUT, "bank search exceeded its deadline");
     }
+    std::fill(b->in_use.begin(), b->in_use.end(), -1);
     if ((st = b->cuda(e, "bank search"))) return st;
     // The compaction wrote the lists in the caller's order, each sorted by
     // (level, bin); offsets are by caller index.

@@ -108,6 +108,8 @@ def test_host_deadline_expiry_then_next_run_succeeds():
     with pytest.raises(B.BrpError) as e:
         bank.run(wl.templates, wl.series_of)
     assert e.value.status == 3
+    # an upload now must not touch the buffer the late run may still read
+    bank.set_series(0, wl.series[0])
     bank.set_wait_limits()
     got, _, status = bank.run(wl.templates, wl.series_of)
     assert not status.any()
