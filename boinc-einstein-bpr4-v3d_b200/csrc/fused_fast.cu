@@ -160,6 +160,20 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     const uint32_t L1 = a.L1, n = a.n, M = a.M, steps = P.steps;
     const float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
 
+    // The rows of the CTA one resident wave ahead (MINB CTAs per SM) into L2,
+    // so that its row loads find them there instead of in HBM.
+    if (threadIdx.x < SEQ) {
+        uint32_t nsm;
+        asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+        const uint64_t lin = uint64_t(blockIdx.y) * gridDim.x + blockIdx.x + uint64_t(nsm) * MINB;
+        if (lin < uint64_t(gridDim.x) * gridDim.y) {
+            const uint32_t qy = uint32_t(lin / gridDim.x), qx = uint32_t(lin % gridDim.x);
+            const float2* row = a.work + size_t(qy) * a.work_stride + size_t(pass2_row(threadIdx.x, R, qx, L1)) * L2;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(uint32_t(L2 * sizeof(float2)))
+                         : "memory");
+        }
+    }
+
     if constexpr (FIRST) {
         // thread t: sequence t / (L2/16), butterfly j = t % (L2/16), inputs j + r L2/16
         constexpr int NBF = L2 / 16;
