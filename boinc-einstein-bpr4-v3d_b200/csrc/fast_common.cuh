@@ -10,6 +10,8 @@
 //  * (int)((double)index + 0.5) as trunc(fl_toward_zero(index + 0.5)): with
 //    every integer below 2^24 representable, rounding toward zero never crosses
 //    an integer, so truncating the rounded sum equals truncating the exact one.
+// In the reference's FMA forms two samples go through packed FP32 instructions
+// together (lean_index2), with the fractional part taken as y - floor(y).
 // The reference-order function brp_resample_index (resample_math.h) remains the
 // definition; tests compare both against the CPU resampler bit for bit.
 #pragma once
@@ -143,6 +145,102 @@ __device__ __forceinline__ int lean_index(uint32_t i, const brp_resample_consts&
     return __float2int_rz(__fadd_rz(index, 0.5f));
 }
 
+// Packed FP32 operations of sm_100: two lanes per instruction, each lane the
+// IEEE operation of the scalar form with the named rounding.
+#define BRP_F2_OP2(name, op)                                                                      \
+    __device__ __forceinline__ float2 name(float2 a, float2 b) {                                  \
+        float2 r;                                                                                 \
+        asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t" op      \
+            " d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"                                                \
+            : "=f"(r.x), "=f"(r.y)                                                                \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                            \
+        return r;                                                                                 \
+    }
+BRP_F2_OP2(add2_rn, "add.rn.f32x2")
+BRP_F2_OP2(add2_rz, "add.rz.f32x2")
+BRP_F2_OP2(add2_rm, "add.rm.f32x2")
+BRP_F2_OP2(mul2_rn, "mul.rn.f32x2")
+#undef BRP_F2_OP2
+
+__device__ __forceinline__ float2 fma2_rn(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{\n\t.reg .b64 a, b, c, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\tmov.b64 c, {%6, %7};\n\t"
+        "fma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+
+// lean_index<true> (the reference's FMA forms) of two samples in packed
+// operations, each step issued once for both samples.  The compiler fuses a
+// packed multiply with a following packed add even when both carry an explicit
+// rounding (CUDA 12.9), so this form is only bit-identical because none of its
+// steps is such a pair: every product feeds an FMA as a factor, or (y, whose
+// floor is taken too) has a second use.  The reference-order arithmetic has
+// such pairs and stays scalar.  The bit-exact index tests run this form at
+// n = 2^21 and 2^22 for every compiled pass-1 configuration.  Differences from
+// the scalar form, each exact:
+//  * a - b as a + (-b), and -(x y) as (-x) y;
+//  * the fractional part y - trunc(y), plus 1 when negative, as
+//    fl(y - floor(y)): y - trunc(y) is exact, and for y < 0 (not an integer)
+//    y - floor(y) is that value plus 1, the same real number rounded once.
+template <bool SMALL = false>
+__device__ __forceinline__ int2 lean_index2(uint32_t i0, uint32_t i1, const brp_resample_consts& p) {
+    float2 fi;
+    if (SMALL)
+        fi = add2_rn(make_float2(__int_as_float(0x4B000000 | int(i0)), __int_as_float(0x4B000000 | int(i1))),
+                     f2(-8388608.0f));
+    else
+        fi = make_float2(u2f_exact<false>(i0), u2f_exact<false>(i1));
+    const float2 t = mul2_rn(fi, f2(p.dt));
+    const float2 ph = fma2_rn(f2(p.omega), t, f2(p.psi));
+    const float2 y = mul2_rn(f2(BRP_INV_TWO_PI_F), ph);
+    const float2 xt = add2_rn(y, make_float2(-floorf(y.x), -floorf(y.y)));
+    const float2 x64 = fma2_rn(xt, f2(64.0f), f2(0.5f));
+    const float2 mg = add2_rm(x64, f2(8388608.0f));
+    const int li0 = __float_as_int(mg.x) - 0x4B000000, li1 = __float_as_int(mg.y) - 0x4B000000;
+    const float2 fli = add2_rn(mg, f2(-8388608.0f));
+    const uint2 sc0 = reinterpret_cast<const uint2*>(c_fast_lut_bits)[li0];
+    const uint2 sc1 = reinterpret_cast<const uint2*>(c_fast_lut_bits)[li1];
+    const float2 s = make_float2(__uint_as_float(sc0.x), __uint_as_float(sc1.x));
+    const float2 c = make_float2(__uint_as_float(sc0.y), __uint_as_float(sc1.y));
+    const float2 d = mul2_rn(f2(BRP_TWO_PI_F), fma2_rn(neg2(fli), f2(0.015625f), xt));
+    const float2 d2 = mul2_rn(mul2_rn(f2(0.5f), d), d);
+    const float2 sn = fma2_rn(neg2(d2), s, fma2_rn(d, c, s));
+    const float2 off = fma2_rn(mul2_rn(f2(p.tau), sn), f2(p.step_inv), f2(-p.s0));
+    const float2 r = add2_rz(add2_rn(fi, neg2(off)), f2(0.5f));
+    return make_int2(__float2int_rz(r.x), __float2int_rz(r.y));
+}
+
+// Source indices j0, j1 of the adjacent samples ib and ib + 1 (the two reals of
+// one complex point) in the index arithmetic MODE selects: -1 for a sample at
+// or past the resampled length, and for one whose index falls outside the
+// series, which also sets oob.
+template <int MODE>
+__device__ __forceinline__ void index_pair(uint32_t ib, const brp_resample_consts& rc, uint32_t steps,
+                                           uint32_t unpadded, int& j0, int& j1, bool& oob) {
+    constexpr bool SMALL = (MODE & kSmallIndex) != 0;
+    j0 = j1 = -1;
+    if (ib < steps) {
+        int2 jj;
+        if constexpr ((MODE & 3) == 2)
+            jj = make_int2(brp_resample_index_fp64(ib, rc), brp_resample_index_fp64(ib + 1, rc));
+        else if constexpr ((MODE & 3) == 1)
+            jj = lean_index2<SMALL>(ib, ib + 1, rc);
+        else
+            jj = make_int2(lean_index<false, SMALL>(ib, rc), lean_index<false, SMALL>(ib + 1, rc));
+        if (uint32_t(jj.x) < unpadded) j0 = jj.x;
+        else oob = true;
+        if (ib + 1 < steps) {
+            if (uint32_t(jj.y) < unpadded) j1 = jj.y;
+            else oob = true;
+        }
+    }
+}
+
 __device__ __forceinline__ brp_resample_consts consts_of(const brp_params& p) {
     brp_resample_consts c;
     c.tau = p.tau; c.omega = p.omega; c.psi = p.psi; c.dt = p.dt; c.step_inv = p.step_inv; c.s0 = p.s0;
@@ -222,17 +320,8 @@ __device__ __forceinline__ double gather(float2* sm, const float* __restrict__ i
     for (int q0 = 0; q0 < PER; q0 += BATCH) {
         int j[2 * BATCH];
 #pragma unroll
-        for (int b = 0; b < 2 * BATCH; ++b) {
-            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
-            j[b] = -1;
-            if (ib < steps) {
-                int jj;
-                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
-                if (uint32_t(jj) < unpadded) j[b] = jj;
-                else oob = true;
-            }
-        }
+        for (int b = 0; b < BATCH; ++b)
+            index_pair<MODE>(i + uint32_t(b) * istep, rc, steps, unpadded, j[2 * b], j[2 * b + 1], oob);
         float v[2 * BATCH];
 #pragma unroll
         for (int b = 0; b < 2 * BATCH; ++b) v[b] = j[b] >= 0 ? __ldg(in + j[b]) : 0.f;
@@ -276,17 +365,8 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
     for (int q = 0; q < 2; ++q) {
         int jx[16];
 #pragma unroll
-        for (int b = 0; b < 16; ++b) {
-            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
-            jx[b] = -1;
-            if (ib < steps) {
-                int jj;
-                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
-                if (uint32_t(jj) < unpadded) jx[b] = jj;
-                else oob = true;
-            }
-        }
+        for (int b = 0; b < 8; ++b)
+            index_pair<MODE>(i + uint32_t(b) * istep, rc, steps, unpadded, jx[2 * b], jx[2 * b + 1], oob);
         float v[16];
 #pragma unroll
         for (int b = 0; b < 16; ++b) v[b] = jx[b] >= 0 ? __ldg(in + jx[b]) : 0.f;

@@ -81,6 +81,17 @@ __device__ __forceinline__ void factor_values(float* v, const float* stage, cons
     }
 }
 
+// s[r] += t[r] for the 16 trial bins, two bins per packed FP32 add (each lane
+// the scalar IEEE add, so the sums are those of the fixed scalar order).
+__device__ __forceinline__ void add_bins(float (&s)[16], const float (&t)[16]) {
+#pragma unroll
+    for (int r = 0; r < 16; r += 2) {
+        const float2 y = __fadd2_rn(make_float2(s[r], s[r + 1]), make_float2(t[r], t[r + 1]));
+        s[r] = y.x;
+        s[r + 1] = y.y;
+    }
+}
+
 // Adds factor K's values to t[r] (or sets them when SET) in the fixed order.
 template <int K, bool SET>
 __device__ __forceinline__ void add_factor(float (&t)[16], const float* stage, const int* doff,
@@ -97,10 +108,14 @@ __device__ __forceinline__ void add_factor(float (&t)[16], const float* stage, c
     } else {
         factor_values<K>(v, stage, doff, Pw, mp, m);
     }
+    float x[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-        const float x = v[(r * K + 8) >> 4];
-        t[r] = SET ? x : t[r] + x;
+    for (int r = 0; r < 16; ++r) x[r] = v[(r * K + 8) >> 4];
+    if constexpr (SET) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) t[r] = x[r];
+    } else {
+        add_bins(t, x);
     }
 }
 
@@ -247,8 +262,7 @@ __device__ __forceinline__ void sums_abc(const HCtx& c, const float (&p16)[16], 
     // stage B: s4 = s2 + (P12 + P4)
     add_factor<12, true>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<4, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
-#pragma unroll
-    for (int r = 0; r < 16; ++r) s[r] += t[r];
+    add_bins(s, t);
     masked<ALLV>(c, s, v);
     level_local<2, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[2], sm2, c.count, c.out, c.cap, c.status,
                          head[1], tail[1]);
@@ -257,8 +271,7 @@ __device__ __forceinline__ void sums_abc(const HCtx& c, const float (&p16)[16], 
     add_factor<10, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<6, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<2, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
-#pragma unroll
-    for (int r = 0; r < 16; ++r) s[r] += t[r];
+    add_bins(s, t);
     masked<ALLV>(c, s, v);
     level_local<3, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[3], sm3, c.count, c.out, c.cap, c.status,
                          head[2], tail[2]);
@@ -278,8 +291,7 @@ __device__ __forceinline__ void sums_d(const HCtx& c, float (&s)[16], LevelTail&
     add_factor<5, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<3, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
     add_factor<1, false>(t, c.stage, c.doff, c.Pw, c.mp, c.m, c.direct, c.M);
-#pragma unroll
-    for (int r = 0; r < 16; ++r) s[r] += t[r];
+    add_bins(s, t);
     masked<ALLV>(c, s, v);
     level_local<4, ALLV>(v, c.i0, c.own, c.fundamental, c.window, c.thr[4], sm4, c.count, c.out, c.cap, c.status,
                          head, tail);

@@ -60,17 +60,8 @@ __device__ __forceinline__ float gather16(float2 (&x)[16], const float* __restri
     for (int q = 0; q < 2; ++q) {
         int jx[16];
 #pragma unroll
-        for (int b = 0; b < 16; ++b) {
-            const uint32_t ib = i + uint32_t(b >> 1) * istep + uint32_t(b & 1);
-            jx[b] = -1;
-            if (ib < steps) {
-                int jj;
-                if ((MODE & 3) == 2) jj = brp_resample_index_fp64(ib, rc);
-                else jj = lean_index<(MODE & 3) == 1, (MODE & kSmallIndex) != 0>(ib, rc);
-                if (uint32_t(jj) < unpadded) jx[b] = jj;
-                else oob = true;
-            }
-        }
+        for (int b = 0; b < 8; ++b)
+            index_pair<MODE>(i + uint32_t(b) * istep, rc, steps, unpadded, jx[2 * b], jx[2 * b + 1], oob);
         float v[16];
 #pragma unroll
         for (int b = 0; b < 16; ++b) v[b] = jx[b] >= 0 ? __ldg(in + jx[b]) : 0.f;
