@@ -45,14 +45,15 @@ __host__ __device__ constexpr int ct_stride(int L, int G) {
 
 template <int R> struct TwStride { static constexpr int value = (R + 1) & ~1; };
 
+// v[r] *= W_{Ns R}^{r k} (r = 1..R-1) from the pass's table (pair (r, r + 1)
+// of butterfly k at 16-byte entry ((r - 1)/2) Ns + k).
 template <int R, int Ns>
 __device__ __forceinline__ void ct_twiddle(float2* v, const float2* __restrict__ tw, int k) {
     if constexpr (Ns > 1) {
-        constexpr int RS = TwStride<R>::value;
-        const float4* w4 = reinterpret_cast<const float4*>(tw + k * RS);
+        const float4* w4 = reinterpret_cast<const float4*>(tw) + k;
 #pragma unroll
         for (int r = 1; r < R; r += 2) {
-            const float4 w = __ldg(w4 + (r - 1) / 2);
+            const float4 w = __ldg(w4 + ((r - 1) / 2) * Ns);
             v[r] = cmul(v[r], make_float2(w.x, w.y));
             if (r + 1 < R) v[r + 1] = cmul(v[r + 1], make_float2(w.z, w.w));
         }

@@ -47,8 +47,10 @@ static const FastPass* find_fast(const std::vector<FastPass>& v, uint32_t L, int
 }
 
 // Per-pass twiddle table of a radix sequence: pass p (span Ns = product of the
-// earlier radices, radix R) holds W_{Ns R}^{r k} at [k * RS + r - 1], RS = R
-// rounded up to even; the first pass (Ns = 1) needs none.
+// earlier radices, radix R) holds the pairs (W_{Ns R}^{(2h+1) k}, W_{Ns R}^{(2h+2) k})
+// (h < RS/2, RS = R rounded up to even, W^0 in the slots past R - 1) as one 16-byte
+// entry at [h Ns + k]: the butterflies of a warp read adjacent k of one pair, so
+// their loads are contiguous.  The first pass (Ns = 1) needs none.
 static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
     uint64_t Ns = 1;
     size_t at = 0;
@@ -59,7 +61,7 @@ static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
                 for (uint64_t r = 0; r < RS; ++r) {
                     const uint64_t e = (r + 1 < R) ? ((r + 1) * k) % (Ns * R) : 0;
                     const double ang = -2.0 * M_PI * (double(e) / double(Ns * R));
-                    out[at + k * RS + r] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
+                    out[at + 2 * ((r / 2) * Ns + k) + (r % 2)] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
                 }
         if (Ns > 1) at += Ns * RS;
         Ns *= R;
