@@ -352,6 +352,7 @@ const std::vector<FastPass>& fast_pass2_configs() {
         P2<512, 4, 256, 4, 8, 8, 8>::info(203),
         P2<2048, 2, 512, 2, 16, 16, 8>::info(204),
         P2<512, 8, 512, 2, 8, 8, 8>::info(205),
+        P2<2048, 4, 1024, 1, 16, 16, 8>::info(207),
     };
     return v;
 }
