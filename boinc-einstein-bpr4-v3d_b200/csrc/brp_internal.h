@@ -9,6 +9,21 @@
 
 namespace brp {
 
+// Twiddles a compiled Stockham pass of radix R keeps per butterfly k in its
+// table.  In a product table (pass 2) radix 2, 4 and 8 keep W^{p k} for the
+// powers p = 1, 2, 4 below R and the kernels form the other twiddles as
+// products of these; otherwise (pass 1; radix 3 and 16 in either) the table
+// holds every twiddle p = 1 .. R - 1.
+__host__ __device__ constexpr bool pass_twiddle_products(int R, bool prod) {
+    return prod && (R == 2 || R == 4 || R == 8);
+}
+__host__ __device__ constexpr int pass_twiddle_powers(int R, bool prod) {
+    return pass_twiddle_products(R, prod) ? (R == 8 ? 3 : R == 4 ? 2 : 1) : R - 1;
+}
+__host__ __device__ constexpr int pass_twiddle_power(int R, int s, bool prod) {
+    return pass_twiddle_products(R, prod) ? 1 << s : s + 1;
+}
+
 // Radix plan of one shared-memory FFT (mirrors the device struct in fft_device.cuh).
 struct RadixPlanHost {
     int count = 0;

@@ -43,26 +43,54 @@ __host__ __device__ constexpr int ct_stride(int L, int G) {
     return base + pad;
 }
 
-template <int R> struct TwStride { static constexpr int value = (R + 1) & ~1; };
+template <int R, bool PROD = false> struct TwStride {
+    static constexpr int value = (pass_twiddle_powers(R, PROD) + 1) & ~1;
+};
 
-// v[r] *= W_{Ns R}^{r k} (r = 1..R-1) from the pass's table (pair (r, r + 1)
-// of butterfly k at 16-byte entry ((r - 1)/2) Ns + k).
-template <int R, int Ns>
+// v[r] *= W_{Ns R}^{r k} (r = 1..R-1).  The pass's table holds, for butterfly
+// k, the twiddles of pass_twiddle_power, pair h at 16-byte entry h Ns + k.  In
+// a product table (PROD, pass 2) radix 2, 4 and 8 load W^k, W^2k, W^4k and
+// form W^3k, W^5k, W^6k, W^7k by one or two complex products, which trades
+// table loads through L1 for FMA-pipe work; pass 1 (whose radix-8 pass ran
+// faster with its table loads) and radix 3 and 16 load every twiddle.
+template <int R, int Ns, bool PROD = false>
 __device__ __forceinline__ void ct_twiddle(float2* v, const float2* __restrict__ tw, int k) {
     if constexpr (Ns > 1) {
         const float4* w4 = reinterpret_cast<const float4*>(tw) + k;
+        if constexpr (pass_twiddle_products(R, PROD)) {
+            const float4 a = __ldg(w4);
+            const float2 w1 = make_float2(a.x, a.y), w2 = make_float2(a.z, a.w);
+            if constexpr (R == 2) {
+                v[1] = cmul(v[1], w1);
+            } else if constexpr (R == 4) {
+                v[3] = cmul(v[3], cmul(w1, w2));
+                v[1] = cmul(v[1], w1);
+                v[2] = cmul(v[2], w2);
+            } else {
+                const float4 b = __ldg(w4 + Ns);
+                const float2 w4k = make_float2(b.x, b.y), w3 = cmul(w1, w2);
+                v[7] = cmul(v[7], cmul(w3, w4k));
+                v[6] = cmul(v[6], cmul(w2, w4k));
+                v[5] = cmul(v[5], cmul(w1, w4k));
+                v[4] = cmul(v[4], w4k);
+                v[3] = cmul(v[3], w3);
+                v[2] = cmul(v[2], w2);
+                v[1] = cmul(v[1], w1);
+            }
+        } else {
 #pragma unroll
-        for (int r = 1; r < R; r += 2) {
-            const float4 w = __ldg(w4 + ((r - 1) / 2) * Ns);
-            v[r] = cmul(v[r], make_float2(w.x, w.y));
-            if (r + 1 < R) v[r + 1] = cmul(v[r + 1], make_float2(w.z, w.w));
+            for (int r = 1; r < R; r += 2) {
+                const float4 w = __ldg(w4 + ((r - 1) / 2) * Ns);
+                v[r] = cmul(v[r], make_float2(w.x, w.y));
+                if (r + 1 < R) v[r + 1] = cmul(v[r + 1], make_float2(w.z, w.w));
+            }
         }
     }
 }
 
 // One Stockham pass: each thread loads its butterflies' inputs, the CTA
 // synchronises, then each thread twiddles, transforms and stores in place.
-template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, bool PROD = false>
 __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ tw) {
     constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
     float2 v[PER][R];
@@ -83,7 +111,7 @@ __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ 
         if (TOTAL % THREADS == 0 || b < TOTAL) {
             const int c = b / NBF, j = b - c * NBF;
             const int k = j % Ns;
-            ct_twiddle<R, Ns>(v[q], tw, k);
+            ct_twiddle<R, Ns, PROD>(v[q], tw, k);
             dft<R>(v[q]);
             float2* dst = buf + c * STRIDE;
             const int base = (j / Ns) * Ns * R + k;
@@ -94,18 +122,19 @@ __device__ __forceinline__ void ct_pass(float2* buf, const float2* __restrict__ 
     __syncthreads();
 }
 
-template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
+template <bool PROD, int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
 __device__ __forceinline__ void ct_fft(float2* buf, const float2* __restrict__ tw) {
-    ct_pass<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw);
+    ct_pass<L, STRIDE, SEQ, THREADS, Ns, R, PROD>(buf, tw);
     if constexpr (sizeof...(Rest) > 0)
-        ct_fft<L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R>::value : 0));
+        ct_fft<PROD, L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R, PROD>::value : 0));
 }
 
-// Number of float2 entries of the per-pass twiddle table of a radix sequence.
-template <int Ns, int R, int... Rest>
+// Number of float2 entries of the per-pass twiddle table of a radix sequence
+// (PROD: a product table).
+template <bool PROD, int Ns, int R, int... Rest>
 __host__ __device__ constexpr int ct_table_size() {
-    int here = Ns > 1 ? Ns * TwStride<R>::value : 0;
-    if constexpr (sizeof...(Rest) > 0) return here + ct_table_size<Ns * R, Rest...>();
+    int here = Ns > 1 ? Ns * TwStride<R, PROD>::value : 0;
+    if constexpr (sizeof...(Rest) > 0) return here + ct_table_size<PROD, Ns * R, Rest...>();
     else return here;
 }
 

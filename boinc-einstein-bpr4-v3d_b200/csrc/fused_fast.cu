@@ -118,8 +118,8 @@ __device__ __forceinline__ void pass2_pairs(float2* sm, const float2* __restrict
                                             const float2* rl_hi, const float2* rl_lo, uint32_t q, uint32_t L1,
                                             uint32_t n, uint32_t steps) {
     if constexpr (sizeof...(Rest) > 0) {
-        ct_pass<L2, STRIDE, 2 * R, THREADS, Ns, RL>(sm, tw);
-        pass2_pairs<L2, STRIDE, R, THREADS, Ns * RL, Rest...>(sm, tw + (Ns > 1 ? Ns * TwStride<RL>::value : 0), pc,
+        ct_pass<L2, STRIDE, 2 * R, THREADS, Ns, RL, true>(sm, tw);
+        pass2_pairs<L2, STRIDE, R, THREADS, Ns * RL, Rest...>(sm, tw + (Ns > 1 ? Ns * TwStride<RL, true>::value : 0), pc,
                                                             rl_hi, rl_lo, q, L1, n, steps);
     } else {
         static_assert(Ns * RL == L2 && R * Ns == THREADS, "one bin-pair butterfly pair per thread");
@@ -131,8 +131,8 @@ __device__ __forceinline__ void pass2_pairs(float2* sm, const float2* __restrict
             v[i] = sm[r * STRIDE + ct_pos(j + i * NBF)];
             u[i] = sm[(R + r) * STRIDE + ct_pos(jm + i * NBF)];
         }
-        ct_twiddle<RL, Ns>(v, tw, j);
-        ct_twiddle<RL, Ns>(u, tw, jm);
+        ct_twiddle<RL, Ns, true>(v, tw, j);
+        ct_twiddle<RL, Ns, true>(u, tw, jm);
         dft<RL>(v);
         dft<RL>(u);
         const uint32_t arow = q * R + r, brow = L1 - arow;
@@ -216,8 +216,8 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
         return;
     }
     // CTA 0 (row 0 and row L1/2 pair with themselves): all passes in shared memory.
-    if constexpr (FIRST) ct_fft<L2, STRIDE, SEQ, THREADS, 16, Rest...>(sm, a.ptw2);
-    else ct_fft<L2, STRIDE, SEQ, THREADS, 1, R0, Rest...>(sm, a.ptw2);
+    if constexpr (FIRST) ct_fft<true, L2, STRIDE, SEQ, THREADS, 16, Rest...>(sm, a.ptw2);
+    else ct_fft<true, L2, STRIDE, SEQ, THREADS, 1, R0, Rest...>(sm, a.ptw2);
 
     // Thread t keeps row pair r = t % R and visits k2 = t / R + it THREADS / R,
     // so k = qR + r + L1 k2 advances by L1 THREADS / R: W_n^{k steps} comes from
@@ -286,7 +286,7 @@ struct P1 {
         int r[] = {Rs...};
         f.plan.count = int(sizeof...(Rs));
         for (int i = 0; i < f.plan.count; ++i) f.plan.radix[i] = r[i];
-        f.table = ct_table_size<1, Rs...>();
+        f.table = ct_table_size<false, 1, Rs...>();
         return f;
     }
 };
@@ -306,7 +306,7 @@ struct P2 {
         int r[] = {Rs...};
         f.plan.count = int(sizeof...(Rs));
         for (int i = 0; i < f.plan.count; ++i) f.plan.radix[i] = r[i];
-        f.table = ct_table_size<1, Rs...>();
+        f.table = ct_table_size<true, 1, Rs...>();
         return f;
     }
 };

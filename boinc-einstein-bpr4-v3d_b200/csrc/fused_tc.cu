@@ -305,7 +305,7 @@ struct P1T {
         int r[] = {16, Rest...};
         f.plan.count = int(1 + sizeof...(Rest));
         for (int i = 0; i < f.plan.count; ++i) f.plan.radix[i] = r[i];
-        f.table = ct_table_size<1, 16, Rest...>();
+        f.table = ct_table_size<false, 1, 16, Rest...>();
         f.tensor = TERMS;
         return f;
     }

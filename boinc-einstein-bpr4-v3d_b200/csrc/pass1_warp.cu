@@ -195,7 +195,7 @@ struct P1W {
         f.id = id; f.L = Lay::L1; f.group = C; f.threads = 512; f.smem = smem; f.launch = &launch; f.attr = &attr;
         f.plan.count = 3;
         f.plan.radix[0] = 16; f.plan.radix[1] = R2; f.plan.radix[2] = 16;
-        f.table = ct_table_size<1, 16, R2, 16>();
+        f.table = ct_table_size<false, 1, 16, R2, 16>();
         return f;
     }
 };

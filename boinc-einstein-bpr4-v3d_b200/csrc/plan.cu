@@ -47,19 +47,22 @@ static const FastPass* find_fast(const std::vector<FastPass>& v, uint32_t L, int
 }
 
 // Per-pass twiddle table of a radix sequence: pass p (span Ns = product of the
-// earlier radices, radix R) holds the pairs (W_{Ns R}^{(2h+1) k}, W_{Ns R}^{(2h+2) k})
-// (h < RS/2, RS = R rounded up to even, W^0 in the slots past R - 1) as one 16-byte
-// entry at [h Ns + k]: the butterflies of a warp read adjacent k of one pair, so
-// their loads are contiguous.  The first pass (Ns = 1) needs none.
-static void fill_pass_tables(float2* out, const RadixPlanHost& plan) {
+// earlier radices, radix R) holds, for butterfly k, the twiddles W_{Ns R}^{q k}
+// of the powers q = pass_twiddle_power(R, s), s < pass_twiddle_powers(R) (W^0
+// in a padding slot to an even count RS), pair h = s / 2 as one 16-byte entry at
+// [h Ns + k]: the butterflies of a warp read adjacent k of one pair, so their
+// loads are contiguous.  The first pass (Ns = 1) needs none.  prod: a product
+// table (pass 2).
+static void fill_pass_tables(float2* out, const RadixPlanHost& plan, bool prod) {
     uint64_t Ns = 1;
     size_t at = 0;
     for (int p = 0; p < plan.count; ++p) {
-        const uint64_t R = plan.radix[p], RS = (R + 1) & ~uint64_t(1);
+        const int R = plan.radix[p], NP = pass_twiddle_powers(R, prod);
+        const uint64_t RS = (uint64_t(NP) + 1) & ~uint64_t(1);
         if (Ns > 1)
             for (uint64_t k = 0; k < Ns; ++k)
                 for (uint64_t r = 0; r < RS; ++r) {
-                    const uint64_t e = (r + 1 < R) ? ((r + 1) * k) % (Ns * R) : 0;
+                    const uint64_t e = (int(r) < NP) ? (uint64_t(pass_twiddle_power(R, int(r), prod)) * k) % (Ns * R) : 0;
                     const double ang = -2.0 * M_PI * (double(e) / double(Ns * R));
                     out[at + 2 * ((r / 2) * Ns + k) + (r % 2)] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
                 }
@@ -175,8 +178,8 @@ void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, floa
     fill_twiddles(host + off[4], uint32_t(off[5] - off[4]), n, 0, split);
     fill_twiddles(host + off[5], split, n, 0, 1);
     if (with_plain) fill_twiddles(host + off[6], lp.B, lp.B, 0, 1);
-    if (lp.fp1) fill_pass_tables(host + off[7], lp.plan1);
-    if (lp.fp2) fill_pass_tables(host + off[8], lp.plan2);
+    if (lp.fp1) fill_pass_tables(host + off[7], lp.plan1, false);
+    if (lp.fp2) fill_pass_tables(host + off[8], lp.plan2, true);
     fill_twiddles(host + off[9], uint32_t(off[10] - off[9]), 2ull * n, 0, split);
     fill_twiddles(host + off[10], split, 2ull * n, 0, 1);
     lp.tw1 = dev + off[0];
