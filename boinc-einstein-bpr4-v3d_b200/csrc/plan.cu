@@ -80,7 +80,7 @@ static void preferred_pair(uint32_t M, int& id1, int& id2) {
     if (M == (1u << 19)) { id1 = 120; id2 = 202; }
     if (M == (3u << 19)) { id1 = 119; id2 = 202; }
     if (M == (1u << 21)) { id1 = 124; id2 = 202; }
-    if (M == (3u << 20)) { id1 = 119; id2 = 204; }
+    if (M == (3u << 20)) { id1 = 119; id2 = 207; }
 }
 
 std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2, bool use_cache) {
