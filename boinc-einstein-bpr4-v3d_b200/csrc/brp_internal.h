@@ -52,6 +52,7 @@ struct LengthPlan {
     const FastPass* fp2 = nullptr;
     const float2 *ptw1 = nullptr, *ptw2 = nullptr;
     const float2 *hf_hi = nullptr, *hf_lo = nullptr;  // W_{2n}^e (cos, -sin of pi e / n)
+    const float2* hq = nullptr;  // W_{4 L2}^e, e < L2: W_{2n}^{L1 e}, the row factor of pass 2's W_{2n}^k
     float2* d_tables = nullptr;
     size_t tables_bytes = 0;
     const float2 *tw1 = nullptr, *tw2 = nullptr, *fs_hi = nullptr, *fs_lo = nullptr, *rl_hi = nullptr,
@@ -74,7 +75,8 @@ bool cached_plan(uint32_t n, CachedPlan& out);
 // with_plain adds the table of the step-by-step pipeline) and the table fill
 // (host[] laid out by the layout, lp's views pointed at dev).
 std::string choose_length_plan(uint32_t n, LengthPlan& plan, int fast1 = 0, int fast2 = 0, bool use_cache = true);
-size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t offsets[12]);
+constexpr int kPlanTableBlocks = 12;  // table blocks of a length plan (length_plan_layout)
+size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t offsets[kPlanTableBlocks + 1]);
 void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, float2* dev);
 void free_length_plan(LengthPlan& plan);
 
@@ -114,6 +116,7 @@ struct FusedArgs {
     const float2 *tw1, *tw2, *fs_hi, *fs_lo, *rl_hi, *rl_lo;
     const float2 *ptw1, *ptw2;  // per-pass twiddle tables of the compiled passes
     const float2 *hf_hi, *hf_lo;  // W_{2n}^e: (cos(pi e/n), -sin(pi e/n)), e <= M
+    const float2* hq;             // W_{4 L2}^e = W_{2n}^{L1 e}, e < L2
     float2* work;     // per template: M complex (four-step intermediate)
     size_t work_stride;
     float* power;     // per template: M floats (P[k] = |X_k|^2 / n, P[0] = 0)

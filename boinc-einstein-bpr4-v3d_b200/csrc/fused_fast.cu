@@ -72,9 +72,12 @@ __device__ __forceinline__ uint32_t pass2_row(int rr, int R, uint32_t q, uint32_
 
 // Real-spectrum post-process of one bin pair k (row arow = k mod L1, arow != 0)
 // and km = M - k: X_k and X_{M-k} from Z_k, Z_{M-k}, the padding term and the
-// normalised power.  wa = W_n^{k steps}.
+// normalised power.  wa = W_n^{k steps}; hf = W_{2n}^k, formed by the caller
+// as W_{2n}^{arow} W_{4 L2}^{k2} (k = arow + L1 k2, 2n = 4 L1 L2): one
+// two-level table value per thread and the row factor hq[k2], read at
+// adjacent k2 by adjacent butterflies.
 struct PostArgs {
-    const float2 *hf_hi, *hf_lo;
+    const float2 *hf_hi, *hf_lo, *hq;
     float* Pw;
     float2* fft;
     float inv_n, fn, hm;  // 1/n, n, -mean/2
@@ -82,9 +85,8 @@ struct PostArgs {
 };
 
 __device__ __forceinline__ void post_pair(const PostArgs& c, uint32_t k, uint32_t km, float2 zk, float2 zm,
-                                          float2 wa) {
-    // cos, sin of pi k / n from the W_2n table; W_n^k = (cos - i sin)^2
-    const float2 hf = twiddle2(c.hf_hi, c.hf_lo, kSplitLog2, k);
+                                          float2 wa, float2 hf) {
+    // cos, sin of pi k / n; W_n^k = (cos - i sin)^2
     const float cv = hf.x, sv = -hf.y;
     const float2 w = make_float2(__fmaf_rn(cv, cv, -sv * sv), -2.f * cv * sv);
     // X_k and X_{M-k} share s = Z_k + Z*_{M-k}, d = Z_k - Z*_{M-k} and t = W d
@@ -137,6 +139,7 @@ __device__ __forceinline__ void pass2_pairs(float2* sm, const float2* __restrict
         dft<RL>(u);
         const uint32_t arow = q * R + r, brow = L1 - arow;
         const float2 wa_step = twiddle2(rl_hi, rl_lo, kSplitLog2, mod_n(uint64_t(L1) * Ns * steps, n));
+        const float2 ha = twiddle2(pc.hf_hi, pc.hf_lo, kSplitLog2, arow);
         float2 wa;
 #pragma unroll
         for (int m = 0; m < RL; ++m) {
@@ -144,7 +147,7 @@ __device__ __forceinline__ void pass2_pairs(float2* sm, const float2* __restrict
             const uint32_t k = arow + L1 * k2, km = brow + L1 * (uint32_t(L2) - 1 - k2);
             if (m % 4 == 0) wa = twiddle2(rl_hi, rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
             else wa = cmul(wa, wa_step);
-            post_pair(pc, k, km, v[m], u[RL - 1 - m], wa);
+            post_pair(pc, k, km, v[m], u[RL - 1 - m], wa, cmul(ha, __ldg(pc.hq + k2)));
         }
     }
 }
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     const bool a_odd = steps & 1u;
     const float pad0 = float(n - steps) * mean;
     PostArgs pc;
-    pc.hf_hi = a.hf_hi; pc.hf_lo = a.hf_lo; pc.Pw = Pw; pc.fft = fft;
+    pc.hf_hi = a.hf_hi; pc.hf_lo = a.hf_lo; pc.hq = a.hq; pc.Pw = Pw; pc.fft = fft;
     pc.inv_n = inv_n; pc.fn = fn; pc.hm = -0.5f * mean; pc.pow2 = pow2; pc.a_odd = a_odd;
 
     if (q > 0) {
@@ -228,6 +231,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
     const int r = threadIdx.x % R;
     const uint32_t arow = q * R + r;
     const float2 wa_step = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(L1) * KSTEP * steps, n));
+    const float2 ha = twiddle2(a.hf_hi, a.hf_lo, kSplitLog2, arow);
     float2 wa;
 #pragma unroll 2
     for (int it = 0; it < ITER; ++it) {
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(THREADS, MINB) pass2_fast(FusedArgs a) {
             const float2 zk = sm[r * STRIDE + ct_pos(k2)], zm = sm[(R + r) * STRIDE + ct_pos(L2 - 1 - k2)];
             if (it % 4 == 0) wa = twiddle2(a.rl_hi, a.rl_lo, kSplitLog2, mod_n(uint64_t(k) * steps, n));
             else wa = cmul(wa, wa_step);
-            post_pair(pc, k, km, zk, zm, wa);
+            post_pair(pc, k, km, zk, zm, wa, cmul(ha, __ldg(a.hq + k2)));
         }
     }
 }

@@ -404,7 +404,7 @@ void fill_fused_args(FusedArgs& a, const LengthPlan& lp) {
     for (int i = 0; i < 6; ++i) { a.plan1[1 + i] = lp.plan1.radix[i]; a.plan2[1 + i] = lp.plan2.radix[i]; }
     a.tw1 = lp.tw1; a.tw2 = lp.tw2; a.fs_hi = lp.fs_hi; a.fs_lo = lp.fs_lo; a.rl_hi = lp.rl_hi; a.rl_lo = lp.rl_lo;
     a.ptw1 = lp.ptw1; a.ptw2 = lp.ptw2;
-    a.hf_hi = lp.hf_hi; a.hf_lo = lp.hf_lo;
+    a.hf_hi = lp.hf_hi; a.hf_lo = lp.hf_lo; a.hq = lp.hq;
     a.wait_polls = kDefaultWaitPolls;
 }
 

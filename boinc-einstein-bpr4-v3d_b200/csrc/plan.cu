@@ -147,28 +147,28 @@ std::string choose_length_plan(uint32_t n, LengthPlan& lp, int fast1, int fast2,
 }
 
 // Table layout of a chosen plan: offsets (float2 entries) of tw1, tw2, fs_hi,
-// fs_lo, rl_hi, rl_lo, twb, ptw1, ptw2, hf_hi, hf_lo and the total.  Tables:
+// fs_lo, rl_hi, rl_lo, twb, ptw1, ptw2, hf_hi, hf_lo, hq and the total.  Tables:
 // tw1[L1] tw2[L2] fs_hi[ceil(M/2048)] fs_lo[2048] rl_hi[ceil(n/2048)] rl_lo[2048]
 // twb[B] (only with_plain) ptw1 ptw2 (per-pass tables of the compiled passes)
 // hf_hi[ceil((M+1)/2048)] hf_lo[2048] (W_{2n}^e = cos(pi e/n) - i sin(pi e/n),
-// e <= M); each block 16-byte aligned.
-size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t off[12]) {
+// e <= M) hq[L2] (W_{4 L2}^e); each block 16-byte aligned.
+size_t length_plan_layout(const LengthPlan& lp, bool with_plain, size_t off[kPlanTableBlocks + 1]) {
     const uint32_t split = 1u << kSplitLog2, n = lp.n;
     const uint32_t fs_hi_n = (lp.M + split - 1) / split, rl_hi_n = (n + split - 1) / split;
     const uint32_t hf_hi_n = (lp.M + 1 + split - 1) / split;
-    const uint32_t counts[11] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, with_plain ? lp.B : 0u,
-                                 uint32_t(lp.fp1 ? lp.fp1->table : 0), uint32_t(lp.fp2 ? lp.fp2->table : 0),
-                                 hf_hi_n, split};
+    const uint32_t counts[kPlanTableBlocks] = {lp.L1, lp.L2, fs_hi_n, split, rl_hi_n, split, with_plain ? lp.B : 0u,
+                                               uint32_t(lp.fp1 ? lp.fp1->table : 0),
+                                               uint32_t(lp.fp2 ? lp.fp2->table : 0), hf_hi_n, split, lp.L2};
     size_t total = 0;
-    for (int i = 0; i < 11; ++i) { off[i] = total; total += (counts[i] + 1) & ~1u; }
-    off[11] = total;
+    for (int i = 0; i < kPlanTableBlocks; ++i) { off[i] = total; total += (counts[i] + 1) & ~1u; }
+    off[kPlanTableBlocks] = total;
     return total;
 }
 
 // Fills the tables of lp into host[] (laid out by length_plan_layout) and
 // points lp's table views at dev (the device copy of host[]).
 void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, float2* dev) {
-    size_t off[12];
+    size_t off[kPlanTableBlocks + 1];
     length_plan_layout(lp, with_plain, off);
     const uint32_t split = 1u << kSplitLog2, n = lp.n;
     if (lp.L1) fill_twiddles(host + off[0], lp.L1, lp.L1, 0, 1);
@@ -182,6 +182,7 @@ void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, floa
     if (lp.fp2) fill_pass_tables(host + off[8], lp.plan2, true);
     fill_twiddles(host + off[9], uint32_t(off[10] - off[9]), 2ull * n, 0, split);
     fill_twiddles(host + off[10], split, 2ull * n, 0, 1);
+    if (lp.L2) fill_twiddles(host + off[11], lp.L2, 4ull * lp.L2, 0, 1);
     lp.tw1 = dev + off[0];
     lp.tw2 = dev + off[1];
     lp.fs_hi = dev + off[2];
@@ -193,12 +194,13 @@ void fill_length_plan_tables(LengthPlan& lp, bool with_plain, float2* host, floa
     lp.ptw2 = dev + off[8];
     lp.hf_hi = dev + off[9];
     lp.hf_lo = dev + off[10];
+    lp.hq = dev + off[11];
 }
 
 std::string make_length_plan(uint32_t n, LengthPlan& lp, cudaStream_t stream, int fast1, int fast2) {
     std::string e = choose_length_plan(n, lp, fast1, fast2);
     if (!e.empty()) return e;
-    size_t off[12];
+    size_t off[kPlanTableBlocks + 1];
     const size_t total = length_plan_layout(lp, true, off);
     lp.tables_bytes = total * sizeof(float2);
     if (cudaMalloc(&lp.d_tables, lp.tables_bytes) != cudaSuccess) return "cudaMalloc of twiddle tables failed";

@@ -129,12 +129,12 @@ extern "C" int brp_cuda_search_static(const brp_params* params, const float* inp
         std::string e = choose_length_plan(p.n, lp, 0, 0, false);  // the built-in plan: no plan file read here
         if (!e.empty()) return static_fail(BRP_E_RUNTIME, e.c_str());
         if (!lp.fused) return static_fail(BRP_E_ARGUMENT, "no fused plan for this length");
-        size_t off[12];
+        size_t off[kPlanTableBlocks + 1];
         if (length_plan_layout(lp, false, off) > kTableEntries || lp.blocks1() > kMaxPartials)
             return static_fail(BRP_E_ARGUMENT, "plan exceeds the static scratch");
         fill_length_plan_tables(lp, false, g_static_host_tables, tables);
-        if (cudaMemcpyAsync(tables, g_static_host_tables, off[11] * sizeof(float2), cudaMemcpyHostToDevice, s) !=
-            cudaSuccess)
+        if (cudaMemcpyAsync(tables, g_static_host_tables, off[kPlanTableBlocks] * sizeof(float2),
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
             return static_fail(BRP_E_RUNTIME, "upload of the twiddle tables failed");
         d.lp = lp;
         d.table_n = p.n;
