@@ -425,18 +425,22 @@ __device__ __forceinline__ double gather_dft16(float2* sm, const float* __restri
 //     T[k1][c0 + c] = Y[c][k1] W_M^{(c0 + c) k1}.
 // Butterfly b of the pass takes column c = b % SEQ and j = b / SEQ, so a warp
 // stores 32/SEQ rows of SEQ adjacent columns; its outputs are rows k1 = j + m Ns.
-// The twiddle comes from the two-level table for m = 0 and m = 4 and in
-// between from the product with W_M^{(c0 + c) Ns} (at most three FP32 complex
-// products from a table value).
+// The twiddle is W_M^{n2 j} W_M^{n2 m Ns} (n2 = c0 + c): one two-level table
+// value per butterfly times the CTA's column factors, computed once into shared
+// memory (rows padded by one entry, so the columns a warp reads sit on
+// distinct banks).  Every thread of the CTA calls this; it synchronises the CTA.
 template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
 __device__ __forceinline__ void ct_last_pass_store(const float2* buf, const float2* __restrict__ tw,
                                                    float2* __restrict__ T, const float2* fs_hi, const float2* fs_lo,
                                                    uint32_t L2, uint32_t c0) {
     constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = (TOTAL + THREADS - 1) / THREADS;
     static_assert(Ns * R == L && THREADS % SEQ == 0, "last-pass tiling");
+    __shared__ float2 s_fs[SEQ][R + 1];
+    for (int t = threadIdx.x; t < SEQ * R; t += THREADS)
+        s_fs[t / R][t % R] = twiddle2(fs_hi, fs_lo, kSplitLog2, (c0 + uint32_t(t / R)) * uint32_t((t % R) * Ns));
+    __syncthreads();
     const int c = threadIdx.x % SEQ;
     const uint32_t n2 = c0 + uint32_t(c);
-    const float2 step = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(Ns));
     const float2* src = buf + c * STRIDE;
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
@@ -447,13 +451,9 @@ __device__ __forceinline__ void ct_last_pass_store(const float2* buf, const floa
         for (int r = 0; r < R; ++r) v[r] = src[ct_pos(j + r * NBF)];
         ct_twiddle<R, Ns>(v, tw, j);
         dft<R>(v);
-        float2 w;
+        const float2 base = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(j));
 #pragma unroll
-        for (int m = 0; m < R; ++m) {
-            if (m % 4 == 0) w = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(j + m * Ns));
-            else w = cmul(w, step);
-            T[size_t(j + m * Ns) * L2 + n2] = cmul(v[m], w);
-        }
+        for (int m = 0; m < R; ++m) T[size_t(j + m * Ns) * L2 + n2] = cmul(v[m], cmul(base, s_fs[c][m]));
     }
 }
 

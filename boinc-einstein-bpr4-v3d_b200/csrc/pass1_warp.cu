@@ -87,12 +87,18 @@ __global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
     constexpr int L1 = Lay::L1, NBF = L1 / 16, MB = 16 / R2;  // MB middle butterflies per lane
     extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[16];
+    __shared__ float2 s_fs[C][17];  // W_M^{n2 m NBF}, n2 = c0 + column, m = 0..15 (rows padded: columns on distinct banks)
     const int g = blockIdx.y;
     const brp_params& P = a.params[g];
     const float* __restrict__ in = a.inputs[g];
     const uint32_t L2 = a.L2, c0 = blockIdx.x * C;
     float* raw = (g == a.snap) ? a.snap_raw : nullptr;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the column factors of the four-step twiddle (read after the block barrier)
+    if (threadIdx.x < 16 * C) {
+        const int col = threadIdx.x / 16, mm = threadIdx.x % 16;
+        s_fs[col][mm] = twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, (c0 + uint32_t(col)) * uint32_t(mm * NBF));
+    }
     const int c = lane % C, q = lane / C;
 
     // ---- gather + first radix-16 pass (butterfly j = w + 16 q of column c)
@@ -161,14 +167,12 @@ __global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
         ct_twiddle<16, NBF>(v, a.ptw1 + 16 * TwStride<R2>::value, jp);
         dft16(v);
         float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
-        const float2 step = twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, n2 * uint32_t(NBF));
-        float2 tw;
+        // W_M^{n2 (jp + m NBF)} = W_M^{n2 jp} W_M^{n2 m NBF}: one table value per
+        // thread and the CTA's column factors from shared memory
+        const float2 base = twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, n2 * uint32_t(jp));
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            if (m % 4 == 0) tw = twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, n2 * uint32_t(jp + m * NBF));
-            else tw = cmul(tw, step);
-            T[size_t(jp + m * NBF) * L2 + n2] = cmul(v[m], tw);
-        }
+        for (int m = 0; m < 16; ++m)
+            T[size_t(jp + m * NBF) * L2 + n2] = cmul(v[m], cmul(base, s_fs[cc][m]));
     }
 
     // ---- this CTA's FP64 sum of its samples; the template's mean from its last CTA
