@@ -1,4 +1,4 @@
-// Pass 1 with warp-local exchanges (compiled pass-1 configurations 124, 125).
+// Pass 1 with warp-local exchanges (compiled pass-1 configurations 124-127).
 //
 // Same transform as pass1_fast with the radix sequence (16, R2, 16) over
 // L1 = 256 R2 and C = 32 / R2 columns per CTA (512 threads): resampling gather
@@ -24,6 +24,18 @@
 // So a CTA synchronises once between the gather and the store (plus the
 // publication of its FP64 sum at the end), and a warp runs its gather, first
 // and middle passes independently of the other warps of its CTA.
+//
+// Configurations 126 and 127 are 124 and 125 with the store of T done by the
+// tensor-memory accelerator: the CTA's outputs form one L1 x C tile of T (rows
+// of C complex values, 8 C bytes, at a row pitch of L2), which the threads
+// write into shared memory (a warp's stores are 256 contiguous bytes there)
+// and one thread sends to T as R2 boxes of 256 rows (cp.async.bulk.tensor,
+// no multicast).  A row of the tile is 32 or 64 bytes, so every st.global of
+// the plain store touches 32/C lines; the bulk store moves the tile without
+// the load/store unit.  The tile reuses the exchange buffer after a barrier.
+#include <cuda.h>  // CUtensorMap; encoded through the runtime's driver entry point (no libcuda link)
+#include <cudaTypedefs.h>
+#include "async_device.cuh"
 #include "fast_common.cuh"
 
 namespace brp {
@@ -81,8 +93,11 @@ __device__ __forceinline__ float gather16(float2 (&x)[16], const float* __restri
     return sum;
 }
 
-template <int R2, int C, int MINB>
-__global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
+// The kernel body; TMA: the store of T as bulk tensor copies through the
+// tensor map *tm (3-D: L2 complex values as 8-byte elements, L1 rows, the
+// launch's templates; box C x 256 x 1).
+template <int R2, int C, bool TMA>
+__device__ __forceinline__ void pass1_warp_body(const FusedArgs& a, const CUtensorMap* tm) {
     using Lay = WarpLayout<R2, C>;
     constexpr int L1 = Lay::L1, NBF = L1 / 16, MB = 16 / R2;  // MB middle butterflies per lane
     extern __shared__ __align__(16) float2 sm[];
@@ -166,13 +181,36 @@ __global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
         for (int r = 0; r < 16; ++r) v[r] = sm[Lay::base(r, cc) + off];
         ct_twiddle<16, NBF>(v, a.ptw1 + 16 * TwStride<R2>::value, jp);
         dft16(v);
-        float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
         // W_M^{n2 (jp + m NBF)} = W_M^{n2 jp} W_M^{n2 m NBF}: one table value per
         // thread and the CTA's column factors from shared memory
         const float2 base = twiddle2(a.fs_hi, a.fs_lo, kSplitLog2, n2 * uint32_t(jp));
+        if constexpr (!TMA) {
+            float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
 #pragma unroll
-        for (int m = 0; m < 16; ++m)
-            T[size_t(jp + m * NBF) * L2 + n2] = cmul(v[m], cmul(base, s_fs[cc][m]));
+            for (int m = 0; m < 16; ++m)
+                T[size_t(jp + m * NBF) * L2 + n2] = cmul(v[m], cmul(base, s_fs[cc][m]));
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = cmul(v[m], cmul(base, s_fs[cc][m]));
+            __syncthreads();  // every thread has read its last-pass inputs from the exchange buffer
+            // the tile [row][column] at the first 128-byte boundary of the buffer
+            // (L1 C 8 = 64 KiB; the buffer has at least 128 bytes more)
+            const uint32_t sm0 = smem_u32(sm), tile_sh = (sm0 + 127u) & ~127u;
+            float2* tile = sm + (tile_sh - sm0) / 8;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) tile[(jp + m * NBF) * C + cc] = v[m];
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the bulk copies
+            __syncthreads();
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int b = 0; b < L1 / 256; ++b)
+                    asm volatile(
+                        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
+                        "r"(int(c0)), "r"(256 * b), "r"(g), "r"(tile_sh + uint32_t(b) * 256u * C * 8u)
+                        : "memory");
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            }
+        }
     }
 
     // ---- this CTA's FP64 sum of its samples; the template's mean from its last CTA
@@ -182,17 +220,66 @@ __global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
         for (int k = 0; k < 16; ++k) tot += red[k];
     }
     publish_mean<512>(a, g, P.steps, tot, red);
+    // the tile stays in shared memory until the bulk copies have read it
+    if constexpr (TMA)
+        if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 template <int R2, int C, int MINB>
+__global__ void __launch_bounds__(512, MINB) pass1_warp(FusedArgs a) {
+    pass1_warp_body<R2, C, false>(a, nullptr);
+}
+
+template <int R2, int C, int MINB>
+__global__ void __launch_bounds__(512, MINB) pass1_warp_tma(FusedArgs a, const __grid_constant__ CUtensorMap tm) {
+    pass1_warp_body<R2, C, true>(a, &tm);
+}
+
+// cuTensorMapEncodeTiled from the driver the runtime has loaded (null if absent).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+template <int R2, int C, int MINB, bool TMA = false>
 struct P1W {
     using Lay = WarpLayout<R2, C>;
     static constexpr int smem = Lay::SLOTS * 8;
+    static_assert(!TMA || smem >= Lay::L1 * C * 8 + 128, "the tile and its alignment fit the exchange buffer");
     static void launch(const FusedArgs& a, uint32_t blocks, uint32_t count, cudaStream_t s) {
-        pass1_warp<R2, C, MINB><<<dim3(blocks, count), 512, smem, s>>>(a);
+        if constexpr (!TMA) {
+            pass1_warp<R2, C, MINB><<<dim3(blocks, count), 512, smem, s>>>(a);
+        } else {
+            // T of the launch's templates: a.work + g work_stride, rows of L2
+            // complex values.  Every box lies inside it (rows 256 b.. < L1,
+            // columns c0.. < L2, c0 8 bytes a multiple of 32).
+            CUtensorMap tm;
+            const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+            const cuuint64_t dim[3] = {a.L2, a.L1, count};
+            const cuuint64_t stride[2] = {cuuint64_t(a.L2) * 8u, cuuint64_t(a.work_stride) * 8u};
+            const cuuint32_t box[3] = {uint32_t(C), 256u, 1u}, estride[3] = {1u, 1u, 1u};
+            const bool ok = enc && a.L1 == uint32_t(Lay::L1) && blocks * uint32_t(C) == a.L2 && count > 0 &&
+                            (reinterpret_cast<uintptr_t>(a.work) & 15u) == 0 &&
+                            enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, a.work, dim, stride, box, estride,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+            // without a tensor map nothing is launched, and the empty grid makes
+            // the caller's launch check report cudaErrorInvalidConfiguration
+            pass1_warp_tma<R2, C, MINB><<<ok ? dim3(blocks, count) : dim3(0, 0), 512, smem, s>>>(a, tm);
+        }
     }
     static cudaError_t attr() {
-        return cudaFuncSetAttribute(pass1_warp<R2, C, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if constexpr (!TMA)
+            return cudaFuncSetAttribute(pass1_warp<R2, C, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        else
+            return cudaFuncSetAttribute(pass1_warp_tma<R2, C, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     }
     static FastPass info(int id) {
         FastPass f;
@@ -209,6 +296,8 @@ struct P1W {
 void append_pass1_warp_configs(std::vector<FastPass>& v) {
     v.push_back(P1W<8, 4, 2>::info(124));  // L1 = 2048 = 16 x 8 x 16, 4 columns (the layout of 110)
     v.push_back(P1W<4, 8, 2>::info(125));  // L1 = 1024 = 16 x 4 x 16, 8 columns (the layout of 118)
+    v.push_back(P1W<8, 4, 2, true>::info(126));  // 124 with the bulk tensor store of T
+    v.push_back(P1W<4, 8, 2, true>::info(127));  // 125 with the bulk tensor store of T
 }
 
 }  // namespace brp

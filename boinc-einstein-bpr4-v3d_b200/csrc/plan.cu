@@ -79,7 +79,7 @@ static void preferred_pair(uint32_t M, int& id1, int& id2) {
     id1 = id2 = 0;
     if (M == (1u << 19)) { id1 = 120; id2 = 202; }
     if (M == (3u << 19)) { id1 = 119; id2 = 202; }
-    if (M == (1u << 21)) { id1 = 124; id2 = 202; }
+    if (M == (1u << 21)) { id1 = 126; id2 = 202; }
     if (M == (3u << 20)) { id1 = 119; id2 = 207; }
 }
 
