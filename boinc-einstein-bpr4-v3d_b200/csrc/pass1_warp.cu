@@ -260,7 +260,7 @@ struct P1W {
             // T of the launch's templates: a.work + g work_stride, rows of L2
             // complex values.  Every box lies inside it (rows 256 b.. < L1,
             // columns c0.. < L2, c0 8 bytes a multiple of 32).
-            CUtensorMap tm;
+            CUtensorMap tm{};
             const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
             const cuuint64_t dim[3] = {a.L2, a.L1, count};
             const cuuint64_t stride[2] = {cuuint64_t(a.L2) * 8u, cuuint64_t(a.work_stride) * 8u};
