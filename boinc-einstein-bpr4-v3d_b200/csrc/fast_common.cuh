@@ -470,5 +470,64 @@ __device__ __forceinline__ void ct_fft_store(float2* buf, const float2* __restri
     }
 }
 
+// ct_last_pass_store with the outputs written as the CTA's L x SEQ tile of T
+// ([row][column], at the first 128-byte boundary of buf) instead of to T: the
+// butterflies of all of a thread's iterations are transformed into registers,
+// the CTA synchronises (every read of buf done), the tile is written (a warp's
+// 32 stores of one output are 256 contiguous bytes) and fenced for the
+// asynchronous proxy, and after a second barrier the caller's one thread sends
+// it to T by bulk tensor copies (tma_store.cuh).  Returns the tile's address.
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R>
+__device__ __forceinline__ uint32_t ct_last_pass_tile(float2* buf, const float2* __restrict__ tw,
+                                                      const float2* fs_hi, const float2* fs_lo, uint32_t c0) {
+    constexpr int NBF = L / R, TOTAL = NBF * SEQ, PER = TOTAL / THREADS;
+    static_assert(Ns * R == L && THREADS % SEQ == 0 && TOTAL % THREADS == 0, "last-pass tiling");
+    __shared__ float2 s_fs[SEQ][R + 1];
+    for (int t = threadIdx.x; t < SEQ * R; t += THREADS)
+        s_fs[t / R][t % R] = twiddle2(fs_hi, fs_lo, kSplitLog2, (c0 + uint32_t(t / R)) * uint32_t((t % R) * Ns));
+    __syncthreads();
+    const int c = threadIdx.x % SEQ;
+    const uint32_t n2 = c0 + uint32_t(c);
+    const float2* src = buf + c * STRIDE;
+    float2 v[PER][R];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int j = threadIdx.x / SEQ + q * (THREADS / SEQ);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q][r] = src[ct_pos(j + r * NBF)];
+        ct_twiddle<R, Ns>(v[q], tw, j);
+        dft<R>(v[q]);
+        const float2 base = twiddle2(fs_hi, fs_lo, kSplitLog2, n2 * uint32_t(j));
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[q][m] = cmul(v[q][m], cmul(base, s_fs[c][m]));
+    }
+    __syncthreads();
+    const uint32_t buf_sh = static_cast<uint32_t>(__cvta_generic_to_shared(buf));
+    const uint32_t tile_sh = (buf_sh + 127u) & ~127u;
+    float2* tile = buf + (tile_sh - buf_sh) / 8;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int j = threadIdx.x / SEQ + q * (THREADS / SEQ);
+#pragma unroll
+        for (int m = 0; m < R; ++m) tile[(j + m * Ns) * SEQ + c] = v[q][m];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    return tile_sh;
+}
+
+// ct_fft_store with the last pass as ct_last_pass_tile; returns the tile's address.
+template <int L, int STRIDE, int SEQ, int THREADS, int Ns, int R, int... Rest>
+__device__ __forceinline__ uint32_t ct_fft_tile(float2* buf, const float2* __restrict__ tw, const float2* fs_hi,
+                                                const float2* fs_lo, uint32_t c0) {
+    if constexpr (sizeof...(Rest) == 0) {
+        return ct_last_pass_tile<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw, fs_hi, fs_lo, c0);
+    } else {
+        ct_pass<L, STRIDE, SEQ, THREADS, Ns, R>(buf, tw);
+        return ct_fft_tile<L, STRIDE, SEQ, THREADS, Ns * R, Rest...>(buf, tw + (Ns > 1 ? Ns * TwStride<R>::value : 0),
+                                                                     fs_hi, fs_lo, c0);
+    }
+}
+
 }  // namespace
 }  // namespace brp

@@ -9,12 +9,15 @@
 // radix-16 butterfly of the first pass, that pass runs in registers inside the
 // gather (gather_dft16), one shared-memory round trip and barrier fewer.
 #include "fast_common.cuh"
+#include "tma_store.cuh"
 
 namespace brp {
 namespace {
 
-template <int L1, int C, int THREADS, int MINB, int R0, int... Rest>
-__global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
+// The pass-1 body; TMA: T is stored as the CTA's tile by bulk tensor copies
+// through *tm (tma_store.cuh) instead of by the threads.
+template <bool TMA, int L1, int C, int THREADS, int R0, int... Rest>
+__device__ __forceinline__ void pass1_fast_body(const FusedArgs& a, const CUtensorMap* tm) {
     constexpr int STRIDE = ct_stride(L1, C);
     constexpr bool FIRST = R0 == 16 && L1 * C == 16 * THREADS;  // first pass fused into the gather
     extern __shared__ __align__(16) float2 sm[];
@@ -44,9 +47,29 @@ __global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
     const double tot = block_sum_d<THREADS>(sum, red);
     publish_mean<THREADS>(a, g, P.steps, tot, red);
 
-    float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
-    if constexpr (FIRST) ct_fft_store<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
-    else ct_fft_store<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
+    if constexpr (!TMA) {
+        float2* __restrict__ T = a.work + size_t(g) * a.work_stride;
+        if constexpr (FIRST) ct_fft_store<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
+        else ct_fft_store<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1, T, a.fs_hi, a.fs_lo, L2, c0);
+    } else {
+        uint32_t tile_sh;
+        if constexpr (FIRST) tile_sh = ct_fft_tile<L1, STRIDE, C, THREADS, 16, Rest...>(sm, a.ptw1, a.fs_hi, a.fs_lo, c0);
+        else tile_sh = ct_fft_tile<L1, STRIDE, C, THREADS, 1, R0, Rest...>(sm, a.ptw1, a.fs_hi, a.fs_lo, c0);
+        if (threadIdx.x == 0) {
+            store_tile_bulk<L1, C>(tm, tile_sh, c0, g);
+            wait_tile_read();  // the tile stays in shared memory until the copies have read it
+        }
+    }
+}
+
+template <int L1, int C, int THREADS, int MINB, int R0, int... Rest>
+__global__ void __launch_bounds__(THREADS, MINB) pass1_fast(FusedArgs a) {
+    pass1_fast_body<false, L1, C, THREADS, R0, Rest...>(a, nullptr);
+}
+
+template <int L1, int C, int THREADS, int MINB, int R0, int... Rest>
+__global__ void __launch_bounds__(THREADS, MINB) pass1_fast_tma(FusedArgs a, const __grid_constant__ CUtensorMap tm) {
+    pass1_fast_body<true, L1, C, THREADS, R0, Rest...>(a, &tm);
 }
 
 __device__ __forceinline__ uint32_t mod_n(uint64_t x, uint32_t n) {
@@ -294,6 +317,28 @@ struct P1 {
         return f;
     }
 };
+// P1 with the bulk tensor store of T (pass1_fast_tma).
+template <int L1, int C, int THREADS, int MINB, int... Rs>
+struct P1T {
+    static constexpr int smem = C * ct_stride(L1, C) * 8;
+    static_assert(smem >= L1 * C * 8 + 128 && L1 % 256 == 0 && C % 2 == 0, "the tile fits the buffer; whole boxes");
+    static void launch(const FusedArgs& a, uint32_t blocks, uint32_t count, cudaStream_t s) {
+        CUtensorMap tm{};
+        const bool ok = encode_tile_map(&tm, a, uint32_t(L1), uint32_t(C), blocks, count);
+        // without a tensor map nothing is launched, and the empty grid makes
+        // the caller's launch check report cudaErrorInvalidConfiguration
+        pass1_fast_tma<L1, C, THREADS, MINB, Rs...><<<ok ? dim3(blocks, count) : dim3(0, 0), THREADS, smem, s>>>(a, tm);
+    }
+    static cudaError_t attr() {
+        return cudaFuncSetAttribute(pass1_fast_tma<L1, C, THREADS, MINB, Rs...>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    static FastPass info(int id) {
+        FastPass f = P1<L1, C, THREADS, MINB, Rs...>::info(id);
+        f.launch = &launch; f.attr = &attr;
+        return f;
+    }
+};
 template <int L2, int R, int THREADS, int MINB, int... Rs>
 struct P2 {
     static constexpr int smem = 2 * R * ct_stride(L2, R) * 8;
@@ -340,6 +385,7 @@ static std::vector<FastPass> make_pass1_configs() {
         P1<2048, 8, 1024, 1, 16, 8, 16>::info(123),
     };
     append_pass1_warp_configs(v);
+    v.push_back(P1T<1536, 4, 384, 2, 16, 4, 3, 8>::info(128));  // 119 with the bulk tensor store of T
     append_pass1_tc_configs(v);
     return v;
 }

@@ -33,10 +33,8 @@
 // no multicast).  A row of the tile is 32 or 64 bytes, so every st.global of
 // the plain store touches 32/C lines; the bulk store moves the tile without
 // the load/store unit.  The tile reuses the exchange buffer after a barrier.
-#include <cuda.h>  // CUtensorMap; encoded through the runtime's driver entry point (no libcuda link)
-#include <cudaTypedefs.h>
-#include "async_device.cuh"
 #include "fast_common.cuh"
+#include "tma_store.cuh"
 
 namespace brp {
 namespace {
@@ -195,21 +193,13 @@ __device__ __forceinline__ void pass1_warp_body(const FusedArgs& a, const CUtens
             __syncthreads();  // every thread has read its last-pass inputs from the exchange buffer
             // the tile [row][column] at the first 128-byte boundary of the buffer
             // (L1 C 8 = 64 KiB; the buffer has at least 128 bytes more)
-            const uint32_t sm0 = smem_u32(sm), tile_sh = (sm0 + 127u) & ~127u;
-            float2* tile = sm + (tile_sh - sm0) / 8;
+            const uint32_t tile_sh = tile_address(sm);
+            float2* tile = sm + (tile_sh - smem_u32(sm)) / 8;
 #pragma unroll
             for (int m = 0; m < 16; ++m) tile[(jp + m * NBF) * C + cc] = v[m];
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the bulk copies
             __syncthreads();
-            if (threadIdx.x == 0) {
-#pragma unroll
-                for (int b = 0; b < L1 / 256; ++b)
-                    asm volatile(
-                        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
-                        "r"(int(c0)), "r"(256 * b), "r"(g), "r"(tile_sh + uint32_t(b) * 256u * C * 8u)
-                        : "memory");
-                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-            }
+            if (threadIdx.x == 0) store_tile_bulk<L1, C>(tm, tile_sh, c0, g);
         }
     }
 
@@ -222,7 +212,7 @@ __device__ __forceinline__ void pass1_warp_body(const FusedArgs& a, const CUtens
     publish_mean<512>(a, g, P.steps, tot, red);
     // the tile stays in shared memory until the bulk copies have read it
     if constexpr (TMA)
-        if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        if (threadIdx.x == 0) wait_tile_read();
 }
 
 template <int R2, int C, int MINB>
@@ -235,19 +225,6 @@ __global__ void __launch_bounds__(512, MINB) pass1_warp_tma(FusedArgs a, const _
     pass1_warp_body<R2, C, true>(a, &tm);
 }
 
-// cuTensorMapEncodeTiled from the driver the runtime has loaded (null if absent).
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }();
-    return fn;
-}
-
 template <int R2, int C, int MINB, bool TMA = false>
 struct P1W {
     using Lay = WarpLayout<R2, C>;
@@ -257,19 +234,8 @@ struct P1W {
         if constexpr (!TMA) {
             pass1_warp<R2, C, MINB><<<dim3(blocks, count), 512, smem, s>>>(a);
         } else {
-            // T of the launch's templates: a.work + g work_stride, rows of L2
-            // complex values.  Every box lies inside it (rows 256 b.. < L1,
-            // columns c0.. < L2, c0 8 bytes a multiple of 32).
             CUtensorMap tm{};
-            const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-            const cuuint64_t dim[3] = {a.L2, a.L1, count};
-            const cuuint64_t stride[2] = {cuuint64_t(a.L2) * 8u, cuuint64_t(a.work_stride) * 8u};
-            const cuuint32_t box[3] = {uint32_t(C), 256u, 1u}, estride[3] = {1u, 1u, 1u};
-            const bool ok = enc && a.L1 == uint32_t(Lay::L1) && blocks * uint32_t(C) == a.L2 && count > 0 &&
-                            (reinterpret_cast<uintptr_t>(a.work) & 15u) == 0 &&
-                            enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, a.work, dim, stride, box, estride,
-                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+            const bool ok = encode_tile_map(&tm, a, uint32_t(Lay::L1), uint32_t(C), blocks, count);
             // without a tensor map nothing is launched, and the empty grid makes
             // the caller's launch check report cudaErrorInvalidConfiguration
             pass1_warp_tma<R2, C, MINB><<<ok ? dim3(blocks, count) : dim3(0, 0), 512, smem, s>>>(a, tm);

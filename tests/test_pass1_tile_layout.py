@@ -1,5 +1,5 @@
 """CPU model of the bulk tensor store of pass 1 (configurations 126 and 127,
-csrc/pass1_warp.cu `pass1_warp_tma`).
+csrc/pass1_warp.cu `pass1_warp_tma`; 128, csrc/fused_fast.cu `pass1_fast_tma`).
 
 The kernel's index arithmetic is restated here and checked exhaustively for
 both compiled shapes, so that every shared-memory write and every bulk copy the
@@ -83,9 +83,42 @@ def test_box_coordinates_meet_the_tma_rules(r2, c, cfg, l2):
     assert np.all(ys >= 0) and np.all(ys + 256 <= l1)
 
 
+def ct_stride(L, G):
+    """Exchange-buffer stride of pass1_fast (fast_common.cuh ct_stride)."""
+    base = L + L // 16
+    want = 1 if G >= 16 else 16 // G
+    return base + (want - base) % 16
+
+
+def test_pass1_fast_tile_config_128():
+    """Config 128 = 119 (L1 = 1536 = 16.4.3.8, 4 columns, 384 threads) with the
+    bulk store: the last radix-8 pass (span 192) of ct_last_pass_tile writes
+    thread t's outputs of butterflies j = t/4 + 96 q (q = 0, 1) to
+    tile[(j + 192 m) 4 + t % 4]."""
+    L1, C, THREADS, R = 1536, 4, 384, 8
+    Ns = NBF = L1 // R
+    PER = NBF * C // THREADS
+    assert PER * THREADS == NBF * C and Ns * R == L1
+    t = np.arange(THREADS)
+    c = t % C
+    idx = np.stack([(t // C + q * (THREADS // C) + m * Ns) * C + c for q in range(PER) for m in range(R)])
+    assert np.array_equal(np.sort(idx.ravel()), np.arange(L1 * C))
+    w = idx.reshape(PER * R, THREADS // 32, 32)
+    assert np.all(np.diff(w, axis=2) == 1) and np.all((w[:, :, 0] * 8) % 256 == 0)
+    smem = C * ct_stride(L1, C) * 8
+    assert smem >= L1 * C * 8 + 128 and L1 % 256 == 0
+    for base in range(0, 4096, 16):
+        tile_sh = (base + 127) & ~127
+        assert tile_sh + L1 * C * 8 <= base + smem and (tile_sh - base) % 8 == 0
+    for l2 in (512, 1024, 2048):  # the pass-2 row lengths it pairs with
+        c0 = np.arange(l2 // C) * C
+        assert np.all((c0 * 8) % 16 == 0) and np.all(c0 + C <= l2)
+
+
 def test_compiled_bulk_store_configs_are_listed():
     from brp_b200._lib import fast_configs
     cfg = {i: (L, k) for i, L, k in fast_configs()}
     for r2, c, cid in SHAPES:
         assert cfg[cid] == (256 * r2, 1)  # pass 1, L1 = 256 R2
     assert cfg[124] == (2048, 1) and cfg[125] == (1024, 1)  # the plain-store forms stay compiled
+    assert cfg[128] == (1536, 1) and cfg[119] == (1536, 1)
