@@ -92,3 +92,22 @@ def test_direct_vector_loads_aligned_and_in_bounds(k):
         end = start + loads * width  # one past the last float read
         assert end <= (mp + 1) * 16  # inside the thread's own bound: direct means (m' + 1) 16 <= M
         assert loads * width >= nv(k)
+
+
+def test_direct_load_line_counts():
+    """Lines of 128 bytes a warp's direct loads touch (32 consecutive blocks):
+    a vector load of factor k spans 32 windows k floats apart, so the even
+    factors and the level-0 values touch 312 lines per warp for 72 lines of
+    data; the odd factors' staged reads are 68 conflict-free shared accesses."""
+    touched = data = 0
+    for k in (2, 4, 6, 8, 10, 12, 14, 16):
+        width = 4 if k % 4 == 0 else 2
+        for v in range((nv(k) + width - 1) // width):
+            lines = set()
+            for lane in range(32):
+                a = ((32000 + lane) * k + v * width) * 4
+                lines.update(range(a // 128, (a + 4 * width - 1) // 128 + 1))
+            touched += len(lines)
+        data += (32 * k * 4) // 128
+    assert (touched, data) == (312, 72)
+    assert sum(nv(k) for k in range(1, 17, 2)) == 68
