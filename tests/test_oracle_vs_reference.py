@@ -86,3 +86,42 @@ def test_search_parameters_match_the_reference(oracle, seed):
                       lambda: oracle.ref_search_parameters(n, samples, sample_us, period, tau, psi, f0, fa, window))
         if po is not None:
             assert bytes(po) == bytes(pr)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_pipeline_matches_the_reference(oracle, seed):
+    """The whole CPU path (src/science.cpp:113-120) of the reference's compiled
+    code, with its FFTW stand-in (the FP64 DFT rounded to float), against the
+    oracle's resampling, the same DFT, power, harmonic sums and selection, on a
+    random template over a series with an injected pulsar; the thresholds are
+    lowered to a high quantile of each level so that every level selects.  The
+    reference build's harmonic step is the stand-in for the absent hs_common.c
+    (the same restatement as the oracle's), so the harmonic sums are not an
+    independent check; resampling, power and selection are."""
+    from brp_b200 import synth
+    rng = np.random.default_rng(3000 + seed)
+    n = int(rng.choice([1 << 12, 3 << 11, 1 << 13, 3 << 12, 1 << 14]))
+    unpadded = n - int(rng.integers(1, 40))
+    pul = synth.Pulsar(float(rng.uniform(50.0, 900.0)), float(rng.uniform(600.0, 20000.0)),
+                       float(rng.uniform(0.0, 1.5)), float(rng.uniform(0.0, 6.2)), 0.3, 5, 0.1)
+    x = synth.make_series(unpadded, seed, [pul])
+    p = oracle.ref_parameters(n, unpadded, pul.tau, pul.period, pul.psi, synth.DT)
+    if seed % 2:
+        p = ref_production(p)
+    ref = oracle.ref_reference(x, p)
+    q = O.Params.from_buffer_copy(bytes(p))
+    for h in range(5):  # the same lowered thresholds on both sides
+        lvl = ref["summed"][h * p.fundamental:(h + 1) * p.fundamental]
+        q.threshold[h] = float(np.float32(np.quantile(lvl[p.window:], 0.995)))
+    ref = oracle.ref_reference(x, q)
+    r = oracle.resample(x, q)
+    assert np.array_equal(r.view(np.uint32), ref["resampled"].view(np.uint32))
+    X = oracle.rfft64_c(r)
+    Xf = X.real.astype(np.float32) + 1j * X.imag.astype(np.float32)
+    P = oracle.power_from_fft(Xf.astype(np.complex128), q.n)
+    assert np.array_equal(P.view(np.uint32), ref["power"].view(np.uint32))
+    S = oracle.harmonic(P, q)
+    assert np.array_equal(S.view(np.uint32), ref["summed"].view(np.uint32))
+    c = oracle.select(S, q)
+    assert len(c) > 0 and set(int(v) for v in c["level"]) == set(range(5))
+    assert c.tobytes() == ref["candidates"].tobytes()
