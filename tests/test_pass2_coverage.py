@@ -17,6 +17,7 @@ import pytest
 PASS2 = {201: (1024, 2, 256, 8), 202: (1024, 4, 512, 8), 203: (512, 4, 256, 8), 204: (2048, 2, 512, 8),
          205: (512, 8, 512, 8), 207: (2048, 4, 1024, 8)}
 L1S = (512, 1024, 1536, 2048, 3072)
+FIRST_RADIX = {201: 16, 202: 16, 203: 8, 204: 16, 205: 8, 207: 16}  # first pass of each radix sequence
 
 
 def written_bins(L1, L2, R, THREADS, RL):
@@ -60,3 +61,41 @@ def test_power_bins_written_exactly_once(cfg, L1):
     assert bins.min() == 0 and bins.max() == M - 1
     counts = np.bincount(bins, minlength=M)
     assert np.all(counts == 1), (np.flatnonzero(counts != 1)[:8], M)
+
+
+def pass2_row(rr, R, q, L1):
+    """Row of sequence rr of CTA q (fused_fast.cu pass2_row)."""
+    if rr < R:
+        return q * R + rr
+    ar = q * R + (rr - R)
+    return L1 // 2 if ar == 0 else L1 - ar
+
+
+@pytest.mark.parametrize("R", [2, 4, 8])
+@pytest.mark.parametrize("L1", L1S)
+def test_every_row_loaded_by_exactly_one_cta(R, L1):
+    """The CTAs' 2R rows (R rows and their mirrors) partition the L1 rows of
+    the intermediate; CTA 0 holds the self-paired rows 0 and L1/2."""
+    if L1 % (2 * R):
+        pytest.skip("the plan pairs R row pairs only with L1 divisible by 2R")
+    rows = [pass2_row(rr, R, q, L1) for q in range(L1 // (2 * R)) for rr in range(2 * R)]
+    assert sorted(rows) == list(range(L1))
+    assert {pass2_row(0, R, 0, L1), pass2_row(R, R, 0, L1)} == {0, L1 // 2}
+    for q in range(1, L1 // (2 * R)):  # a mirror row pairs Z_k with Z_{M-k}: row a with row L1 - a
+        for r in range(R):
+            assert pass2_row(r, R, q, L1) + pass2_row(R + r, R, q, L1) == L1
+
+
+@pytest.mark.parametrize("cfg", sorted(PASS2))
+def test_first_pass_row_loads_cover_the_rows(cfg):
+    """With the first radix-16 pass on the loads (2R L2 = 16 THREADS), thread
+    t loads inputs j + r L2/16 (r < 16) of sequence t / (L2/16), j = t % (L2/16):
+    every element of the CTA's 2R rows once."""
+    L2, R, THREADS, _ = PASS2[cfg]
+    if 2 * R * L2 != 16 * THREADS or FIRST_RADIX[cfg] != 16:
+        pytest.skip("this configuration loads its rows in shared memory first")
+    nbf = L2 // 16
+    t = np.arange(THREADS)[:, None]
+    r = np.arange(16)[None, :]
+    elem = (t // nbf) * L2 + (t % nbf) + r * nbf
+    assert np.array_equal(np.sort(elem.ravel()), np.arange(2 * R * L2))
